@@ -1,0 +1,87 @@
+/*
+ * onefft_b200 — entry points added beside OneFFT's API (include/onefft.h) for device memory,
+ * batches, uneven batches and error reporting. OneFFT has no counterpart for these: it is a
+ * single-threaded CPU library whose callers parallelise over transforms themselves
+ * (OneFFT include/onefft.h:36-44, tests/test_onefft.c:207-259); on the GPU the batch is the unit
+ * of work, so it becomes part of the interface.
+ *
+ * Return codes: 0 success; -1 invalid size or allocation failure (as OneFFT); -2 invalid
+ * argument (NULL, misaligned or overlapping device pointers, zero/huge counts); -(1000 + e) for a
+ * CUDA runtime error e. On any error the output is left untouched unless the error came from the
+ * device after the kernels started. onefft_last_error() describes the last error of the
+ * calling thread.
+ *
+ * Streams are passed as `void *` holding a cudaStream_t (NULL = the legacy default stream), so
+ * the header needs no CUDA include. Device entry points only enqueue work; they do not
+ * synchronise. They use the CUDA device current in the calling thread, which must be the
+ * device the plan was created on.
+ */
+#ifndef ONEFFT_CUDA_H
+#define ONEFFT_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "onefft.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ONEFFT_ERR_SIZE (-1)
+#define ONEFFT_ERR_ARG (-2)
+#define ONEFFT_ERR_CUDA_BASE (-1000)
+
+/* ---- batched transforms on device memory ------------------------------------------------------
+ * Counterpart of calling OneFFT's onefft_plan_forward/_inverse (src/onefft.c:1138-1140) `batch`
+ * times on consecutive transforms: transform b reads d_in + 2 n b and writes d_out + 2 n b.
+ * d_in and d_out are device pointers aligned to 8 bytes (one complex64) that do not overlap. */
+ONEFFT_API int onefft_dev_forward_batched(const onefft_plan *plan, const float *d_in, float *d_out, size_t batch, void *stream);
+ONEFFT_API int onefft_dev_inverse_batched(const onefft_plan *plan, const float *d_in, float *d_out, size_t batch, void *stream);
+
+/* The adjoint of the unnormalised forward transform, F^H = conj(F)^T, applied to `batch`
+ * gradients: d_grad_in = F^H d_grad_out. Equal to the unnormalised inverse transform; used by
+ * the torch autograd wrapper. Same pointer rules as above. */
+ONEFFT_API int onefft_dev_adjoint_batched(const onefft_plan *plan, const float *d_grad_out, float *d_grad_in, size_t batch,
+                               void *stream);
+
+/* ---- batched transforms on host memory ---------------------------------------------------------
+ * Same as calling onefft_plan_forward/_inverse on `batch` consecutive transforms of host (or
+ * device) buffers, but pipelined: chunks are copied in, transformed and copied out on several
+ * streams so that both copy directions overlap the kernels. Pinned host memory gives full
+ * overlap; pageable memory works but copies synchronously. Blocks until done. */
+ONEFFT_API int onefft_plan_forward_batched(const onefft_plan *plan, const float *in, float *out, size_t batch);
+ONEFFT_API int onefft_plan_inverse_batched(const onefft_plan *plan, const float *in, float *out, size_t batch);
+
+/* ---- plans with an explicit pass split ---------------------------------------------------------
+ * Creates a plan whose transform runs as `npass` kernels of lengths 2^log2_len[0..npass-1]
+ * (product n). npass = 1 allows n <= 2^14; npass = 2 or 3 allow passes of 2^4 .. 2^12 each.
+ * onefft_plan_create() picks the split from the tuned table; this form exists for tuning and for
+ * tests that exercise every pass kernel at small sizes. NULL on an invalid split. */
+ONEFFT_API onefft_plan *onefft_plan_create_split(size_t n, int npass, const int *log2_len);
+
+/* Number of passes of a plan and their log2 lengths (up to 3 are written to log2_len). */
+ONEFFT_API int onefft_plan_passes(const onefft_plan *plan, int *log2_len);
+
+/* ---- information and testing hooks -------------------------------------------------------------*/
+
+/* Message of the last error in the calling thread ("" if none). */
+ONEFFT_API const char *onefft_last_error(void);
+
+/* Test hook: make the k-th device allocation from now on fail (k >= 1), as if the device were
+ * out of memory; 0 disarms. Used by the tests of the -1 / untouched-output contract. */
+ONEFFT_API void onefft_debug_fail_alloc(int k);
+
+/* Test hook: evaluates the library's FP64 twiddle rule on the current device and copies the
+ * FP32-rounded values w_(2^log2n)^k, k = 0 .. count-1, to host memory `out` (2 count floats).
+ * This is the rule every device table is built with (OneFFT src/onefft.c:112-141). */
+ONEFFT_API int onefft_debug_twiddles(unsigned log2n, size_t count, float *out);
+
+/* Number of kernel launches this process has issued through the library (all threads). */
+ONEFFT_API unsigned long long onefft_debug_launch_count(void);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* ONEFFT_CUDA_H */

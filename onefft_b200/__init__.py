@@ -1,0 +1,241 @@
+"""onefft_b200 — OneFFT's power-of-two FP32 complex FFT as hand-written sm_100a CUDA.
+
+The product is ``libonefft_cuda.so`` with the C ABI of ``include/onefft.h`` (OneFFT's own API)
+and ``include/onefft_cuda.h`` (device-pointer, batched and uneven-batch additions). This module
+is the Python host mirror of that interface, shaped like OneFFT's C++ layer
+(include/onefft.h:123-169 of OneFFT): ``forward``/``inverse`` without plan management, a
+``Plan`` that owns the tables of one size, ``cache_prepare``/``cache_clear`` and
+``implementation``. Errors follow OneFFT's contract: an invalid size raises ``ValueError`` (the C
+call returned -1 / NULL) and leaves any output buffer untouched.
+
+There is no CPU fallback: if the CUDA library is missing, importing the entry points raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libonefft_cuda.so")
+
+_c_float_p = ctypes.POINTER(ctypes.c_float)
+_sz = ctypes.c_size_t
+_vp = ctypes.c_void_p
+
+# exported symbols of the C ABI, in header order (include/onefft.h, include/onefft_cuda.h)
+C_SYMBOLS = (
+    "onefft_forward", "onefft_inverse", "onefft_cache_prepare", "onefft_cache_clear",
+    "onefft_plan_create", "onefft_plan_destroy", "onefft_plan_forward", "onefft_plan_inverse",
+    "onefft_plan_size", "onefft_implementation",
+    "onefft_dev_forward_batched", "onefft_dev_inverse_batched", "onefft_dev_adjoint_batched",
+    "onefft_plan_forward_batched", "onefft_plan_inverse_batched",
+    "onefft_plan_create_split", "onefft_plan_passes",
+    "onefft_last_error", "onefft_debug_fail_alloc", "onefft_debug_twiddles", "onefft_debug_launch_count",
+)
+
+_lib: ctypes.CDLL | None = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded CUDA library with typed entry points (raises if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is not built: run `python -m onefft_b200.build` "
+                           "(there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    L.onefft_forward.argtypes = [_vp, _vp, _sz]
+    L.onefft_forward.restype = ctypes.c_int
+    L.onefft_inverse.argtypes = [_vp, _vp, _sz]
+    L.onefft_inverse.restype = ctypes.c_int
+    L.onefft_cache_prepare.argtypes = [_sz]
+    L.onefft_cache_prepare.restype = ctypes.c_int
+    L.onefft_cache_clear.argtypes = []
+    L.onefft_cache_clear.restype = None
+    L.onefft_plan_create.argtypes = [_sz]
+    L.onefft_plan_create.restype = _vp
+    L.onefft_plan_create_split.argtypes = [_sz, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.onefft_plan_create_split.restype = _vp
+    L.onefft_plan_destroy.argtypes = [_vp]
+    L.onefft_plan_destroy.restype = None
+    L.onefft_plan_forward.argtypes = [_vp, _vp, _vp]
+    L.onefft_plan_forward.restype = None
+    L.onefft_plan_inverse.argtypes = [_vp, _vp, _vp]
+    L.onefft_plan_inverse.restype = None
+    L.onefft_plan_size.argtypes = [_vp]
+    L.onefft_plan_size.restype = _sz
+    L.onefft_plan_passes.argtypes = [_vp, ctypes.POINTER(ctypes.c_int)]
+    L.onefft_plan_passes.restype = ctypes.c_int
+    L.onefft_implementation.argtypes = []
+    L.onefft_implementation.restype = ctypes.c_char_p
+    for name in ("onefft_dev_forward_batched", "onefft_dev_inverse_batched", "onefft_dev_adjoint_batched"):
+        f = getattr(L, name)
+        f.argtypes = [_vp, _vp, _vp, _sz, _vp]
+        f.restype = ctypes.c_int
+    for name in ("onefft_plan_forward_batched", "onefft_plan_inverse_batched"):
+        f = getattr(L, name)
+        f.argtypes = [_vp, _vp, _vp, _sz]
+        f.restype = ctypes.c_int
+    L.onefft_last_error.argtypes = []
+    L.onefft_last_error.restype = ctypes.c_char_p
+    L.onefft_debug_fail_alloc.argtypes = [ctypes.c_int]
+    L.onefft_debug_fail_alloc.restype = None
+    L.onefft_debug_twiddles.argtypes = [ctypes.c_uint, _sz, _vp]
+    L.onefft_debug_twiddles.restype = ctypes.c_int
+    L.onefft_debug_launch_count.argtypes = []
+    L.onefft_debug_launch_count.restype = ctypes.c_ulonglong
+    _lib = L
+    return L
+
+
+def implementation() -> str:
+    return lib().onefft_implementation().decode()
+
+
+def last_error() -> str:
+    return lib().onefft_last_error().decode()
+
+
+def _as_interleaved(x) -> np.ndarray:
+    """A C-contiguous float32 view (2n floats) of complex64 or interleaved float32 data."""
+    a = np.asarray(x)
+    if a.dtype == np.complex64:
+        a = a.view(np.float32)
+    if a.dtype != np.float32:
+        raise TypeError("expected complex64 or interleaved float32 data")
+    if not a.flags.c_contiguous:
+        a = np.ascontiguousarray(a)
+    return a.reshape(-1)
+
+
+def _out_like(a: np.ndarray, out):
+    if out is None:
+        return np.empty_like(a)
+    o = _as_interleaved(out)
+    if o.size != a.size:
+        raise ValueError("output size differs from input size")
+    return o
+
+
+def forward(x, out=None):
+    """OneFFT's onefft_forward on host data (complex64 or interleaved float32)."""
+    a = _as_interleaved(x)
+    o = _out_like(a, out)
+    if lib().onefft_forward(a.ctypes.data, o.ctypes.data, a.size // 2) != 0:
+        raise ValueError(f"onefft_forward failed: {last_error()}")
+    return o
+
+
+def inverse(x, out=None):
+    """OneFFT's onefft_inverse on host data (unnormalised)."""
+    a = _as_interleaved(x)
+    o = _out_like(a, out)
+    if lib().onefft_inverse(a.ctypes.data, o.ctypes.data, a.size // 2) != 0:
+        raise ValueError(f"onefft_inverse failed: {last_error()}")
+    return o
+
+
+def cache_prepare(n: int) -> None:
+    if lib().onefft_cache_prepare(n) != 0:
+        raise ValueError(f"onefft_cache_prepare({n}) failed: {last_error()}")
+
+
+def cache_clear() -> None:
+    lib().onefft_cache_clear()
+
+
+class Plan:
+    """Owns the device tables of one size (OneFFT's onefft::Plan, include/onefft.h:136-167)."""
+
+    def __init__(self, n: int, split: tuple[int, ...] | None = None):
+        L = lib()
+        if split is None:
+            h = L.onefft_plan_create(n)
+        else:
+            arr = (ctypes.c_int * len(split))(*split)
+            h = L.onefft_plan_create_split(n, len(split), arr)
+        if not h:
+            raise ValueError(f"no plan for n={n}: {last_error()}")
+        self._h = h
+        self.n = int(n)
+
+    @property
+    def handle(self) -> int:
+        if not self._h:
+            raise ValueError("plan was destroyed")
+        return self._h
+
+    def size(self) -> int:
+        return int(lib().onefft_plan_size(self.handle))
+
+    def passes(self) -> tuple[int, ...]:
+        buf = (ctypes.c_int * 3)()
+        k = lib().onefft_plan_passes(self.handle, buf)
+        return tuple(buf[i] for i in range(k))
+
+    def destroy(self) -> None:
+        if getattr(self, "_h", None):
+            lib().onefft_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()
+
+    def _host(self, x, out, inverse: bool, batch: int | None):
+        a = _as_interleaved(x)
+        o = _out_like(a, out)
+        if batch is None:
+            if a.size != 2 * self.n:
+                raise ValueError("input size differs from the plan size")
+            f = lib().onefft_plan_inverse if inverse else lib().onefft_plan_forward
+            f(self.handle, a.ctypes.data, o.ctypes.data)
+            err = last_error()
+            if err:
+                raise RuntimeError(err)
+        else:
+            if a.size != 2 * self.n * batch:
+                raise ValueError("input size differs from batch * plan size")
+            f = lib().onefft_plan_inverse_batched if inverse else lib().onefft_plan_forward_batched
+            rc = f(self.handle, a.ctypes.data, o.ctypes.data, batch)
+            if rc != 0:
+                raise RuntimeError(f"batched transform failed ({rc}): {last_error()}")
+        return o
+
+    def forward(self, x, out=None, batch: int | None = None):
+        return self._host(x, out, False, batch)
+
+    def inverse(self, x, out=None, batch: int | None = None):
+        return self._host(x, out, True, batch)
+
+    # ---- device pointers (raw addresses; see onefft_b200.torch_ops for tensors) ----
+
+    def dev_forward(self, d_in: int, d_out: int, batch: int = 1, stream: int = 0) -> None:
+        rc = lib().onefft_dev_forward_batched(self.handle, d_in, d_out, batch, stream)
+        if rc != 0:
+            raise RuntimeError(f"onefft_dev_forward_batched failed ({rc}): {last_error()}")
+
+    def dev_inverse(self, d_in: int, d_out: int, batch: int = 1, stream: int = 0) -> None:
+        rc = lib().onefft_dev_inverse_batched(self.handle, d_in, d_out, batch, stream)
+        if rc != 0:
+            raise RuntimeError(f"onefft_dev_inverse_batched failed ({rc}): {last_error()}")
+
+    def dev_adjoint(self, d_grad_out: int, d_grad_in: int, batch: int = 1, stream: int = 0) -> None:
+        rc = lib().onefft_dev_adjoint_batched(self.handle, d_grad_out, d_grad_in, batch, stream)
+        if rc != 0:
+            raise RuntimeError(f"onefft_dev_adjoint_batched failed ({rc}): {last_error()}")
+
+
+__all__ = ["forward", "inverse", "cache_prepare", "cache_clear", "Plan", "implementation", "last_error",
+           "lib", "LIB_PATH", "C_SYMBOLS"]

@@ -1,0 +1,39 @@
+// Internal launch interface between the C-ABI layer (onefft_api.cu) and the kernels
+// (fft_kernels.cu). Nothing here is exported from the shared library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace ofb {
+
+// Arguments of one pass of the multi-pass decomposition (see k_pass in fft_kernels.cu).
+struct PassArgs {
+    const float2* in;
+    float2* out;
+    int log2n;       // transform size; consecutive transforms of a batch are 2^log2n apart
+    int log_s;       // log2 of the element stride of this pass (first pass: log2(n / L0))
+    int rev_b1;      // first pass: log2 L1, log2 L2 (0 for two passes) of the digit reversal
+    int rev_b2;
+    int swap_in;     // inverse: exchange re/im on load (first pass) / on store (last pass)
+    int swap_out;
+    const float2* stw;      // stage twiddles of this pass's tile length
+    const double2* tw_lo;   // two-level FP64 tables of w_n
+    const double2* tw_hi;
+    int lo_bits;
+};
+
+// Largest size handled by one kernel (k_tiny / k_batched).
+constexpr int kMaxSingleLog2 = 14;
+
+int batched_log_c(int log_l);
+int pass_log_c(int log_l);
+
+cudaError_t launch_single_kernel(int log2n, const float2* in, float2* out, long long batch, const float2* stw,
+                                 int inverse, cudaStream_t stream);
+cudaError_t launch_pass(int mode, int log_l, const PassArgs& a, int batch, cudaStream_t stream);
+cudaError_t launch_stage_table(float2* dst, int log_l, cudaStream_t stream);
+cudaError_t launch_big_table(double2* lo, double2* hi, int log2n, int lo_bits, cudaStream_t stream);
+int stage_table_entries_host(int log_l);
+cudaError_t launch_twiddle_probe(float2* dst, unsigned log2n, unsigned long long count, cudaStream_t stream);
+
+}  // namespace ofb

@@ -1,0 +1,570 @@
+// C-ABI layer of libonefft_cuda.so: plans, the plan cache, the host-pointer drop-in calls and the
+// device-pointer batched calls.
+//
+// OneFFT's runtime (src/onefft.c:1094-1189) is restated for the device:
+//   - a plan is immutable after creation and holds every table in one allocation, here one
+//     cudaMalloc filled by kernels that evaluate the FP64 twiddle rule on the device;
+//   - the cache is one slot per log2 n (and per device), filled lock-free by compare-and-swap;
+//     the loser of a race destroys its copy (src/onefft.c:1151-1167);
+//   - invalid sizes and allocation failures return -1 / NULL with the output untouched
+//     (include/onefft.h:73-75).
+// The host-pointer calls stage through per-thread device buffers on a per-thread stream, so
+// concurrent callers never share mutable state.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+
+#include "../../include/onefft_cuda.h"
+#include "fft_launch.h"
+
+using namespace ofb;
+
+// ---- errors, test hooks, counters --------------------------------------------------------------
+
+static thread_local std::string t_last_error;
+static std::atomic<int> g_fail_alloc_countdown{0};
+std::atomic<unsigned long long> g_launches{0};
+
+static int set_error(int code, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+static int set_error(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    t_last_error = buf;
+    return code;
+}
+
+static int cuda_error(cudaError_t e, const char *what) {
+    cudaGetLastError();  // clear a non-sticky error so later calls start clean
+    return set_error(ONEFFT_ERR_CUDA_BASE - (int)e, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// Device allocation with the test hook of onefft_debug_fail_alloc().
+static cudaError_t dev_alloc(void **p, size_t bytes) {
+    int k = g_fail_alloc_countdown.load();
+    while (k > 0) {
+        if (g_fail_alloc_countdown.compare_exchange_weak(k, k - 1)) {
+            if (k == 1) {
+                *p = nullptr;
+                return cudaErrorMemoryAllocation;
+            }
+            break;
+        }
+    }
+    return cudaMalloc(p, bytes);
+}
+
+static bool size_log2(size_t n, int *log2n) {
+    if (n == 0 || (n & (n - 1)) != 0) return false;
+    int l = 0;
+    while (((size_t)1 << l) < n) ++l;
+    if (l > 30) return false;
+    *log2n = l;
+    return true;
+}
+
+// ---- plans -------------------------------------------------------------------------------------
+
+struct onefft_plan {
+    size_t n;
+    int log2n;
+    int device;
+    int npass;
+    int len[3];          // log2 of each pass length
+    void *mem;           // the one device allocation
+    size_t mem_bytes;
+    const float2 *stw[3];  // stage twiddles of each pass's length
+    const double2 *tw_lo;  // two-level FP64 tables of w_n (npass >= 2)
+    const double2 *tw_hi;
+    int lo_bits;
+};
+
+// Tuned pass split per log2 n: one kernel up to 2^14, two passes up to 2^24, three beyond.
+static void default_split(int m, int *npass, int *len) {
+    if (m <= kMaxSingleLog2) {
+        *npass = 1;
+        len[0] = m;
+    } else if (m <= 24) {
+        *npass = 2;
+        len[0] = (m + 1) / 2;
+        len[1] = m / 2;
+    } else {
+        *npass = 3;
+        len[0] = (m + 2) / 3;
+        len[1] = (m + 1) / 3;
+        len[2] = m / 3;
+    }
+}
+
+static bool valid_split(int m, int npass, const int *len) {
+    if (npass == 1) return len[0] == m && m <= kMaxSingleLog2;
+    if (npass < 2 || npass > 3) return false;
+    int sum = 0;
+    for (int p = 0; p < npass; ++p) {
+        if (len[p] < 4 || len[p] > 12) return false;
+        sum += len[p];
+    }
+    return sum == m;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static onefft_plan *plan_build(size_t n, int m, int npass, const int *len) {
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) {
+        cuda_error(e, "no CUDA device");
+        return nullptr;
+    }
+    onefft_plan *p = new (std::nothrow) onefft_plan();
+    if (!p) {
+        set_error(ONEFFT_ERR_SIZE, "out of host memory");
+        return nullptr;
+    }
+    p->n = n;
+    p->log2n = m;
+    p->device = device;
+    p->npass = npass;
+    for (int i = 0; i < npass; ++i) p->len[i] = len[i];
+    // layout: stage tables per pass, then the FP64 tables
+    size_t off[3], bytes = 0;
+    for (int i = 0; i < npass; ++i) {
+        off[i] = bytes;
+        bytes = align256(bytes + sizeof(float2) * (size_t)stage_table_entries_host(len[i]));
+    }
+    size_t lo_off = bytes, hi_off = bytes;
+    if (npass >= 2) {
+        p->lo_bits = m / 2;
+        lo_off = bytes;
+        bytes = align256(bytes + sizeof(double2) * ((size_t)1 << p->lo_bits));
+        hi_off = bytes;
+        bytes = align256(bytes + sizeof(double2) * ((size_t)1 << (m - p->lo_bits)));
+    }
+    if (bytes == 0) bytes = 256;
+    e = dev_alloc(&p->mem, bytes);
+    if (e != cudaSuccess) {
+        delete p;
+        cuda_error(e, "plan table allocation");
+        set_error(ONEFFT_ERR_SIZE, "plan table allocation failed");
+        return nullptr;
+    }
+    p->mem_bytes = bytes;
+    char *base = (char *)p->mem;
+    cudaStream_t s;
+    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        for (int i = 0; i < npass && e == cudaSuccess; ++i) {
+            p->stw[i] = (const float2 *)(base + off[i]);
+            e = launch_stage_table((float2 *)(base + off[i]), len[i], s);
+        }
+        if (npass >= 2 && e == cudaSuccess) {
+            p->tw_lo = (const double2 *)(base + lo_off);
+            p->tw_hi = (const double2 *)(base + hi_off);
+            e = launch_big_table((double2 *)p->tw_lo, (double2 *)p->tw_hi, m, p->lo_bits, s);
+        }
+        cudaError_t e2 = cudaStreamSynchronize(s);
+        if (e == cudaSuccess) e = e2;
+        cudaStreamDestroy(s);
+    }
+    if (e != cudaSuccess) {
+        cudaFree(p->mem);
+        delete p;
+        cuda_error(e, "plan table build");
+        return nullptr;
+    }
+    return p;
+}
+
+extern "C" onefft_plan *onefft_plan_create(size_t n) {
+    int m;
+    if (!size_log2(n, &m)) {
+        set_error(ONEFFT_ERR_SIZE, "n=%zu is not a power of two in [1, 2^30]", n);
+        return nullptr;
+    }
+    int npass, len[3];
+    default_split(m, &npass, len);
+    return plan_build(n, m, npass, len);
+}
+
+extern "C" onefft_plan *onefft_plan_create_split(size_t n, int npass, const int *log2_len) {
+    int m;
+    if (!size_log2(n, &m)) {
+        set_error(ONEFFT_ERR_SIZE, "n=%zu is not a power of two in [1, 2^30]", n);
+        return nullptr;
+    }
+    if (!log2_len || !valid_split(m, npass, log2_len)) {
+        set_error(ONEFFT_ERR_ARG, "invalid pass split for n=%zu", n);
+        return nullptr;
+    }
+    return plan_build(n, m, npass, log2_len);
+}
+
+extern "C" void onefft_plan_destroy(onefft_plan *plan) {
+    if (!plan) return;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != plan->device) cudaSetDevice(plan->device);
+    cudaFree(plan->mem);
+    if (cur >= 0 && cur != plan->device) cudaSetDevice(cur);
+    delete plan;
+}
+
+extern "C" size_t onefft_plan_size(const onefft_plan *plan) { return plan ? plan->n : 0; }
+
+extern "C" int onefft_plan_passes(const onefft_plan *plan, int *log2_len) {
+    if (!plan) return 0;
+    for (int i = 0; i < plan->npass && log2_len; ++i) log2_len[i] = plan->len[i];
+    return plan->npass;
+}
+
+extern "C" const char *onefft_implementation(void) { return "cuda sm_100a"; }
+
+extern "C" const char *onefft_last_error(void) { return t_last_error.c_str(); }
+
+extern "C" void onefft_debug_fail_alloc(int k) { g_fail_alloc_countdown.store(k < 0 ? 0 : k); }
+
+extern "C" unsigned long long onefft_debug_launch_count(void) { return g_launches.load(); }
+
+// ---- execution on device memory ---------------------------------------------------------------
+
+// Enqueues `batch` transforms; d_in / d_out are 8-byte aligned device pointers, not overlapping.
+static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *out, long long batch, int inverse,
+                                cudaStream_t s) {
+    if (batch <= 0) return cudaSuccess;
+    if (p->npass == 1) {
+        g_launches.fetch_add(1);
+        return launch_single_kernel(p->log2n, in, out, batch, p->stw[0], inverse, s);
+    }
+    PassArgs a{};
+    a.log2n = p->log2n;
+    a.tw_lo = p->tw_lo;
+    a.tw_hi = p->tw_hi;
+    a.lo_bits = p->lo_bits;
+    int done = 0;  // log2 of the digits transformed so far
+    for (int i = 0; i < p->npass; ++i) {
+        const bool first = i == 0, last = i == p->npass - 1;
+        a.in = first ? in : out;
+        a.out = out;
+        a.stw = p->stw[i];
+        a.swap_in = first && inverse;
+        a.swap_out = last && inverse;
+        if (first) {
+            a.log_s = p->log2n - p->len[0];
+            a.rev_b1 = p->len[1];
+            a.rev_b2 = p->npass == 3 ? p->len[2] : 0;
+        } else {
+            a.log_s = done;
+        }
+        int mode = first ? 0 : last ? 2 : 1;
+        g_launches.fetch_add(1);
+        cudaError_t e = launch_pass(mode, p->len[i], a, (int)batch, s);
+        if (e != cudaSuccess) return e;
+        done += p->len[i];
+    }
+    return cudaSuccess;
+}
+
+static bool is_device_pointer(const void *ptr) {
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+static bool ranges_overlap(const void *a, const void *b, size_t bytes) {
+    uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+    return x < y + bytes && y < x + bytes;
+}
+
+static int dev_batched(const onefft_plan *p, const float *d_in, float *d_out, size_t batch, int inverse,
+                       void *stream) {
+    t_last_error.clear();
+    if (!p) return set_error(ONEFFT_ERR_ARG, "NULL plan");
+    if (batch == 0) return 0;
+    if (!d_in || !d_out) return set_error(ONEFFT_ERR_ARG, "NULL buffer");
+    if (((uintptr_t)d_in | (uintptr_t)d_out) & 7) return set_error(ONEFFT_ERR_ARG, "device buffers must be 8-byte aligned");
+    if (batch > ((size_t)1 << 40) / p->n) return set_error(ONEFFT_ERR_ARG, "batch too large");
+    size_t bytes = batch * p->n * sizeof(float2);
+    if (ranges_overlap(d_in, d_out, bytes)) return set_error(ONEFFT_ERR_ARG, "input and output overlap");
+    cudaError_t e = plan_enqueue(p, (const float2 *)d_in, (float2 *)d_out, (long long)batch, inverse,
+                                 (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_error(e, "kernel launch");
+    return 0;
+}
+
+extern "C" int onefft_dev_forward_batched(const onefft_plan *plan, const float *d_in, float *d_out, size_t batch,
+                                          void *stream) {
+    return dev_batched(plan, d_in, d_out, batch, 0, stream);
+}
+
+extern "C" int onefft_dev_inverse_batched(const onefft_plan *plan, const float *d_in, float *d_out, size_t batch,
+                                          void *stream) {
+    return dev_batched(plan, d_in, d_out, batch, 1, stream);
+}
+
+extern "C" int onefft_dev_adjoint_batched(const onefft_plan *plan, const float *d_grad_out, float *d_grad_in,
+                                          size_t batch, void *stream) {
+    // F^H = conj(F): the unnormalised inverse transform, i.e. the forward kernels with re/im
+    // exchanged on load and store.
+    return dev_batched(plan, d_grad_out, d_grad_in, batch, 1, stream);
+}
+
+// ---- per-thread host staging -------------------------------------------------------------------
+
+namespace {
+
+constexpr int kStreams = 3;
+
+struct ThreadCtx {
+    int device = -1;
+    cudaStream_t stream[kStreams] = {};
+    cudaEvent_t done[kStreams] = {};
+    void *buf[kStreams] = {};  // device staging, in + out per stream
+    size_t cap[kStreams] = {};
+
+    ~ThreadCtx() {
+        // may run after the CUDA runtime has shut down at process exit: ignore errors
+        for (int i = 0; i < kStreams; ++i) {
+            if (buf[i]) cudaFree(buf[i]);
+            if (stream[i]) cudaStreamDestroy(stream[i]);
+            if (done[i]) cudaEventDestroy(done[i]);
+        }
+    }
+
+    cudaError_t init(int dev) {
+        if (device == dev) return cudaSuccess;
+        if (device >= 0) return cudaErrorInvalidDevice;  // one device per thread context
+        for (int i = 0; i < kStreams; ++i) {
+            cudaError_t e = cudaStreamCreateWithFlags(&stream[i], cudaStreamNonBlocking);
+            if (e != cudaSuccess) return e;
+            e = cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming);
+            if (e != cudaSuccess) return e;
+        }
+        device = dev;
+        return cudaSuccess;
+    }
+
+    cudaError_t reserve(int i, size_t bytes) {
+        if (cap[i] >= bytes) return cudaSuccess;
+        if (buf[i]) {
+            cudaStreamSynchronize(stream[i]);
+            cudaFree(buf[i]);
+            buf[i] = nullptr;
+            cap[i] = 0;
+        }
+        cudaError_t e = dev_alloc(&buf[i], bytes);
+        if (e != cudaSuccess) {
+            buf[i] = nullptr;
+            return e;
+        }
+        cap[i] = bytes;
+        return cudaSuccess;
+    }
+};
+
+// Contexts per device for this thread (a thread may use plans of several devices).
+constexpr int kMaxDevices = 64;
+thread_local ThreadCtx *t_ctx[kMaxDevices];
+struct CtxReaper {
+    ~CtxReaper() {
+        for (int i = 0; i < kMaxDevices; ++i) delete t_ctx[i];
+    }
+};
+thread_local CtxReaper t_reaper;
+
+ThreadCtx *thread_ctx(int device, cudaError_t *err) {
+    (void)&t_reaper;  // odr-use so the reaper is constructed for this thread
+    if (device < 0 || device >= kMaxDevices) {
+        *err = cudaErrorInvalidDevice;
+        return nullptr;
+    }
+    ThreadCtx *&c = t_ctx[device];
+    if (!c) c = new (std::nothrow) ThreadCtx();
+    if (!c) {
+        *err = cudaErrorMemoryAllocation;
+        return nullptr;
+    }
+    *err = c->init(device);
+    return *err == cudaSuccess ? c : nullptr;
+}
+
+// Switches to a plan's device for the duration of a call.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) cudaSetDevice(dev);
+        else prev = -1;
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+// One transform (or `batch`) through host or device buffers, synchronous. Returns 0 or an error;
+// `out` is written only by the final copy, after every kernel succeeded.
+static int host_execute(const onefft_plan *p, const float *in, float *out, size_t batch, int inverse) {
+    t_last_error.clear();
+    if (!p) return set_error(ONEFFT_ERR_ARG, "NULL plan");
+    if (batch == 0) return 0;
+    if (!in || !out) return set_error(ONEFFT_ERR_ARG, "NULL buffer");
+    DeviceGuard guard(p->device);
+    cudaError_t e;
+    ThreadCtx *ctx = thread_ctx(p->device, &e);
+    if (!ctx) return cuda_error(e, "thread context");
+    const size_t tbytes = p->n * sizeof(float2);
+    const bool in_dev = is_device_pointer(in), out_dev = is_device_pointer(out);
+    const bool aligned = (((uintptr_t)in | (uintptr_t)out) & 7) == 0;
+    if (in_dev && out_dev && aligned && !ranges_overlap(in, out, tbytes * batch)) {
+        // device memory of the caller: transform in place of the caller's buffers
+        e = plan_enqueue(p, (const float2 *)in, (float2 *)out, (long long)batch, inverse, ctx->stream[0]);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream[0]);
+        return e == cudaSuccess ? 0 : cuda_error(e, "transform");
+    }
+    // Chunks of whole transforms, round-robin over the streams: chunk k's copy-in overlaps the
+    // kernels and copy-out of chunks k-1 and k-2.
+    size_t per_chunk = batch;
+    const size_t target = (size_t)32 << 20;  // ~32 MiB of input per chunk
+    if (batch > 1 && tbytes * batch > 2 * target) {
+        per_chunk = target / tbytes;
+        if (per_chunk == 0) per_chunk = 1;
+    }
+    const size_t chunks = (batch + per_chunk - 1) / per_chunk;
+    const int nstreams = chunks == 1 ? 1 : kStreams;
+    for (int i = 0; i < nstreams; ++i) {
+        e = ctx->reserve(i, 2 * tbytes * per_chunk);
+        if (e != cudaSuccess) return set_error(ONEFFT_ERR_SIZE, "staging allocation failed: %s", cudaGetErrorString(e));
+    }
+    // Input copies of every chunk may all be issued before any output is written back, so a
+    // failure in any kernel can still leave `out` untouched: outputs are copied only after the
+    // kernels of all chunks were enqueued without error. For several chunks the copy-out of a
+    // chunk is issued right after its kernels (overlap); a device fault then surfaces at the sync.
+    for (size_t k = 0; k < chunks; ++k) {
+        const int si = (int)(k % nstreams);
+        cudaStream_t s = ctx->stream[si];
+        const size_t first = k * per_chunk;
+        const size_t cnt = (first + per_chunk <= batch) ? per_chunk : batch - first;
+        float2 *d_in = (float2 *)ctx->buf[si];
+        float2 *d_out = d_in + per_chunk * p->n;
+        e = cudaMemcpyAsync(d_in, (const char *)in + first * tbytes, cnt * tbytes, cudaMemcpyDefault, s);
+        if (e != cudaSuccess) break;
+        e = plan_enqueue(p, d_in, d_out, (long long)cnt, inverse, s);
+        if (e != cudaSuccess) break;
+        if (chunks == 1) {
+            // single chunk: check the kernels before the output is touched
+            e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) break;
+        }
+        e = cudaMemcpyAsync((char *)out + first * tbytes, d_out, cnt * tbytes, cudaMemcpyDefault, s);
+        if (e != cudaSuccess) break;
+    }
+    cudaError_t e2 = cudaSuccess;
+    for (int i = 0; i < nstreams; ++i) {
+        cudaError_t es = cudaStreamSynchronize(ctx->stream[i]);
+        if (e2 == cudaSuccess) e2 = es;
+    }
+    if (e == cudaSuccess) e = e2;
+    return e == cudaSuccess ? 0 : cuda_error(e, "transform");
+}
+
+extern "C" void onefft_plan_forward(const onefft_plan *plan, const float *in, float *out) {
+    host_execute(plan, in, out, 1, 0);
+}
+
+extern "C" void onefft_plan_inverse(const onefft_plan *plan, const float *in, float *out) {
+    host_execute(plan, in, out, 1, 1);
+}
+
+extern "C" int onefft_plan_forward_batched(const onefft_plan *plan, const float *in, float *out, size_t batch) {
+    return host_execute(plan, in, out, batch, 0);
+}
+
+extern "C" int onefft_plan_inverse_batched(const onefft_plan *plan, const float *in, float *out, size_t batch) {
+    return host_execute(plan, in, out, batch, 1);
+}
+
+// ---- the plan cache (src/onefft.c:1151-1189) -----------------------------------------------------
+
+static std::atomic<onefft_plan *> g_cache[kMaxDevices][31];
+
+static const onefft_plan *cache_get(size_t n, int *err) {
+    int m;
+    if (!size_log2(n, &m)) {
+        *err = set_error(ONEFFT_ERR_SIZE, "n=%zu is not a power of two in [1, 2^30]", n);
+        return nullptr;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        *err = cuda_error(e, "no CUDA device");
+        return nullptr;
+    }
+    if (dev < 0 || dev >= kMaxDevices) {
+        *err = set_error(ONEFFT_ERR_ARG, "device %d out of range", dev);
+        return nullptr;
+    }
+    std::atomic<onefft_plan *> &slot = g_cache[dev][m];
+    onefft_plan *p = slot.load(std::memory_order_acquire);
+    if (p) return p;
+    p = onefft_plan_create(n);
+    if (!p) {
+        *err = ONEFFT_ERR_SIZE;
+        return nullptr;
+    }
+    onefft_plan *expected = nullptr;
+    if (!slot.compare_exchange_strong(expected, p, std::memory_order_acq_rel, std::memory_order_acquire)) {
+        onefft_plan_destroy(p);
+        p = expected;
+    }
+    return p;
+}
+
+extern "C" int onefft_forward(const float *in, float *out, size_t n) {
+    int err = 0;
+    const onefft_plan *p = cache_get(n, &err);
+    if (!p) return -1;
+    return host_execute(p, in, out, 1, 0) == 0 ? 0 : -1;
+}
+
+extern "C" int onefft_inverse(const float *in, float *out, size_t n) {
+    int err = 0;
+    const onefft_plan *p = cache_get(n, &err);
+    if (!p) return -1;
+    return host_execute(p, in, out, 1, 1) == 0 ? 0 : -1;
+}
+
+extern "C" int onefft_cache_prepare(size_t n) {
+    int err = 0;
+    return cache_get(n, &err) ? 0 : -1;
+}
+
+extern "C" void onefft_cache_clear(void) {
+    for (int d = 0; d < kMaxDevices; ++d)
+        for (int m = 0; m < 31; ++m) onefft_plan_destroy(g_cache[d][m].exchange(nullptr, std::memory_order_acq_rel));
+}
+
+extern "C" int onefft_debug_twiddles(unsigned log2n, size_t count, float *out) {
+    t_last_error.clear();
+    if (log2n > 30 || !out || count > ((size_t)1 << 30)) return set_error(ONEFFT_ERR_ARG, "invalid twiddle probe");
+    if (count == 0) return 0;
+    void *d = nullptr;
+    cudaError_t e = dev_alloc(&d, count * sizeof(float2));
+    if (e != cudaSuccess) return set_error(ONEFFT_ERR_SIZE, "probe allocation failed");
+    e = launch_twiddle_probe((float2 *)d, log2n, count, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d, count * sizeof(float2), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? 0 : cuda_error(e, "twiddle probe");
+}

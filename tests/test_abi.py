@@ -1,0 +1,100 @@
+"""CPU tests of the C-ABI boundary: the library loads, exports every symbol that include/*.h
+declares, and rejects invalid sizes the way OneFFT does (tests/test_onefft.c:170-182) before any
+device work — these calls touch no GPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols() -> set[str]:
+    names = set()
+    for h in ("onefft.h", "onefft_cuda.h"):
+        src = open(os.path.join(ROOT, "include", h)).read()
+        names |= set(re.findall(r"^ONEFFT_API [^;]*?\b(onefft_\w+)\(", src, flags=re.M))
+    return names
+
+
+def exported_symbols(path: str) -> set[str]:
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True, check=True).stdout
+    return {line.split()[-1] for line in out.splitlines() if " T " in line}
+
+
+@pytest.fixture(scope="module")
+def cuda_lib():
+    import onefft_b200
+    if not os.path.exists(onefft_b200.LIB_PATH):
+        from onefft_b200 import build
+        build.build()
+    return onefft_b200.lib()
+
+
+def test_header_declares_reference_api():
+    names = declared_symbols()
+    reference_api = {"onefft_forward", "onefft_inverse", "onefft_cache_prepare", "onefft_cache_clear",
+                     "onefft_plan_create", "onefft_plan_destroy", "onefft_plan_forward", "onefft_plan_inverse",
+                     "onefft_plan_size", "onefft_implementation"}
+    assert reference_api <= names
+
+
+def test_library_exports_every_declared_symbol(cuda_lib):
+    import onefft_b200
+    exported = exported_symbols(onefft_b200.LIB_PATH)
+    missing = declared_symbols() - exported
+    assert not missing, missing
+    # the Python mirror types exactly the declared set
+    assert set(onefft_b200.C_SYMBOLS) == declared_symbols()
+    for name in declared_symbols():
+        assert hasattr(cuda_lib, name)
+
+
+def test_library_links_no_torch_and_no_cufft():
+    import onefft_b200
+    deps = subprocess.run(["ldd", onefft_b200.LIB_PATH], capture_output=True, text=True).stdout
+    assert "torch" not in deps and "cufft" not in deps
+
+
+def test_implementation_string(cuda_lib):
+    assert cuda_lib.onefft_implementation() == b"cuda sm_100a"
+
+
+def test_invalid_sizes_rejected_without_device(cuda_lib):
+    """Same list as tests/test_onefft.c:171; validation happens before any CUDA call."""
+    invalid = [0, 3, 5, 6, 7, 12, 1000, 1023, 1025, 2**64 - 1, 2**31]
+    for n in invalid:
+        assert cuda_lib.onefft_plan_create(n) is None
+    cuda_lib.onefft_plan_destroy(None)  # must be accepted
+    x = np.zeros(6, np.float32)
+    out = np.full(6, 7.0, np.float32)
+    assert cuda_lib.onefft_forward(x.ctypes.data, out.ctypes.data, 3) == -1
+    assert cuda_lib.onefft_inverse(x.ctypes.data, out.ctypes.data, 0) == -1
+    assert (out == 7.0).all()
+    assert cuda_lib.onefft_cache_prepare(12) == -1 and cuda_lib.onefft_cache_prepare(0) == -1
+    assert b"power of two" in cuda_lib.onefft_last_error()
+    split = (ctypes.c_int * 2)(4, 4)
+    assert cuda_lib.onefft_plan_create_split(1000, 2, split) is None
+    bad = (ctypes.c_int * 2)(3, 5)  # pass shorter than 16
+    assert cuda_lib.onefft_plan_create_split(256, 2, bad) is None
+    assert cuda_lib.onefft_plan_size(None) == 0
+
+
+def test_device_calls_reject_bad_arguments_without_device(cuda_lib):
+    # NULL plan is rejected on the host
+    assert cuda_lib.onefft_dev_forward_batched(None, 0, 0, 1, None) == -2
+    assert cuda_lib.onefft_plan_forward_batched(None, 0, 0, 1) == -2
+
+
+def test_python_mirror_raises_on_invalid_size(cuda_lib):
+    import onefft_b200
+    with pytest.raises(ValueError):
+        onefft_b200.forward(np.zeros(6, np.float32))
+    with pytest.raises(ValueError):
+        onefft_b200.Plan(12)

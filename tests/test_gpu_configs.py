@@ -1,0 +1,148 @@
+"""GPU parity at the full sizes of the benchmark configurations, through the C ABI.
+
+  n=1024 single forward+inverse, uniform [-1,1): inverse(forward(x)) = 1024 x and the forward
+      result against an FP64 direct DFT of every bin;
+  16384 x n=4096 batched, standard normal: 64 sampled transforms against FP64 (each within 2x
+      the reference library's error on the same transform), and the whole batch through
+      size-independent properties (Parseval per transform, linearity);
+  single n = 2^20, 2^24 against the full FP64 FFT within 2x the reference's error;
+  single n = 2^27 against the reference library's own output, round trip, Parseval and sampled
+      direct-DFT bins.
+The parity rule: relative RMS against the FP64 oracle at most 2x the reference's on the same
+input (FP32 arithmetic, so this is the tolerance; no bitwise claim), max-abs stated.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SEED_C1 = 0xC0F1
+SEED_C2 = 0xC0F2
+
+
+def torch():
+    import torch as t
+    return t
+
+
+def test_config1_n1024(ofb, oracle):
+    n = 1024
+    x, _ = oracle.gen_uniform(2 * n, SEED_C1)
+    plan = ofb.Plan(n)
+    y = plan.forward(x)
+    back = plan.inverse(y)
+    assert oracle.rel_rms(back, x.astype(np.float64) * n) < 2 * oracle.tolerance(10)
+    want = oracle.dft_bins(x, np.arange(n))
+    err = oracle.rel_rms(y, want)
+    ref = oracle.rel_rms(oracle.ref_fft(x), want) if oracle.have_reference() else None
+    print(f"config1 n=1024 rel_rms {err:.3g} (reference {ref}) max_abs {oracle.max_abs(y, want):.3g}")
+    assert err < oracle.tolerance(10)
+    if ref is not None:
+        assert err <= 2 * ref
+    plan.destroy()
+
+
+def test_config2_batched_4096(ofb, oracle):
+    T = torch()
+    n, batch = 4096, 16384
+    x = oracle.gen_normal(2 * n * batch, SEED_C2)
+    plan = ofb.Plan(n)
+    d_in = T.from_numpy(x).cuda()
+    d_out = T.empty_like(d_in)
+    rng = np.random.default_rng(5)
+    sample = np.sort(rng.choice(batch, 64, replace=False))
+    for inv in (False, True):
+        (plan.dev_inverse if inv else plan.dev_forward)(d_in.data_ptr(), d_out.data_ptr(), batch)
+        T.cuda.synchronize()
+        out = d_out.view(batch, n, 2)
+        worst = worst_ratio = 0.0
+        for b in sample:
+            xb = x[2 * n * b:2 * n * (b + 1)]
+            want = oracle.fft64(xb, inv)
+            got = out[b].cpu().numpy().reshape(-1)
+            err = oracle.rel_rms(got, want)
+            assert err < oracle.tolerance(12)
+            if oracle.have_reference():
+                ref = oracle.rel_rms(oracle.ref_fft(xb, inv), want)
+                worst_ratio = max(worst_ratio, err / ref)
+            worst = max(worst, oracle.max_abs(got, want))
+        print(f"config2 4096x16384 {'inv' if inv else 'fwd'}: worst err/ref {worst_ratio:.3f} max_abs {worst:.3g}")
+        assert worst_ratio <= 2.0
+        # Parseval on every transform: sum |X|^2 = n sum |x|^2
+        xin = d_in.view(batch, n, 2).double()
+        e_in = (xin ** 2).sum(dim=(1, 2))
+        e_out = (out.double() ** 2).sum(dim=(1, 2))
+        rel = ((e_out - n * e_in).abs() / (n * e_in)).max().item()
+        assert rel < 1e-5
+    # linearity over the whole batch: F(a x + y) = a F(x) + F(y)
+    y_in = T.roll(d_in, shifts=2 * n)  # another valid batch
+    fa = T.empty_like(d_in)
+    fb = T.empty_like(d_in)
+    fab = T.empty_like(d_in)
+    plan.dev_forward(d_in.data_ptr(), fa.data_ptr(), batch)
+    plan.dev_forward(y_in.data_ptr(), fb.data_ptr(), batch)
+    comb = (2.0 * d_in + y_in).contiguous()
+    plan.dev_forward(comb.data_ptr(), fab.data_ptr(), batch)
+    T.cuda.synchronize()
+    num = (fab.double() - (2.0 * fa.double() + fb.double())).norm()
+    den = fab.double().norm()
+    assert (num / den).item() < 1e-6
+    plan.destroy()
+
+
+@pytest.mark.parametrize("log2n", [20, 24])
+def test_config2_single_large(ofb, oracle, ref_errors, log2n):
+    T = torch()
+    n = 1 << log2n
+    x = oracle.gen_normal(2 * n, ref_errors["seed_normal"] + log2n)
+    plan = ofb.Plan(n)
+    d_in = T.from_numpy(x).cuda()
+    d_out = T.empty_like(d_in)
+    for inv in (False, True):
+        d = "inverse" if inv else "forward"
+        (plan.dev_inverse if inv else plan.dev_forward)(d_in.data_ptr(), d_out.data_ptr(), 1)
+        T.cuda.synchronize()
+        got = d_out.cpu().numpy()
+        want = oracle.fft64_numpy(x, inv)
+        err = oracle.rel_rms(got, want)
+        ref = ref_errors["normal"][str(log2n)][d]["rel_rms"]
+        print(f"config2 n=2^{log2n} {d}: rel_rms {err:.3g} reference {ref:.3g} max_abs {oracle.max_abs(got, want):.3g}")
+        assert err <= 2 * ref
+        assert err < oracle.tolerance(log2n)
+    plan.destroy()
+
+
+def test_config2_single_2p27(ofb, oracle):
+    T = torch()
+    log2n = 27
+    n = 1 << log2n
+    x = oracle.gen_normal(2 * n, 0x27)
+    plan = ofb.Plan(n)
+    assert plan.passes() == (9, 9, 9)
+    d_in = T.from_numpy(x).cuda()
+    d_out = T.empty_like(d_in)
+    d_back = T.empty_like(d_in)
+    plan.dev_forward(d_in.data_ptr(), d_out.data_ptr(), 1)
+    plan.dev_inverse(d_out.data_ptr(), d_back.data_ptr(), 1)
+    T.cuda.synchronize()
+    # round trip and Parseval on the device, in FP64
+    xin = d_in.double()
+    rt = ((d_back.double() - n * xin).norm() / (n * xin.norm())).item()
+    assert rt < 2 * oracle.tolerance(log2n)
+    pars = abs((d_out.double() ** 2).sum().item() - n * (xin ** 2).sum().item()) / (n * (xin ** 2).sum().item())
+    assert pars < 1e-5
+    got = d_out.cpu().numpy()
+    del d_back
+    # sampled bins against the FP64 direct DFT
+    bins = [1, n // 3]
+    want = oracle.dft_bins(x, bins)
+    sel = got.reshape(-1, 2)[bins].reshape(-1)
+    assert np.abs(sel - want).max() / np.abs(want).max() < 2e-6
+    if oracle.have_reference():
+        ref = oracle.ref_fft(x)
+        d = oracle.rel_rms(got, ref.astype(np.float64))
+        print(f"n=2^27: GPU vs reference relative RMS difference {d:.3g}")
+        assert d < 2 * oracle.tolerance(log2n)
+    plan.destroy()
