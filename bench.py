@@ -1,33 +1,38 @@
-"""Benchmark of the B200 FFT path: batched FP32 complex FFT, 16384 transforms of n = 4096.
+"""Benchmark of the B200 FFT path on the batched + large-transform workload.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-One step = one forward transform of the whole batch (16384 x 4096 complex64, 512 MiB in and
-512 MiB out, larger than the 126 MB L2, so no flush is needed between steps), launched through
-the C ABI's device-pointer batched entry point on the current torch stream and timed with CUDA
-events over exactly K steps, barrier + synchronize on both sides, max over ranks.
+Workload (per GPU): the batched FP32 complex FFT configuration — 16384 independent transforms of
+n = 4096 (512 MiB interleaved complex64) plus single transforms of n = 2^20, 2^24 and 2^27 —
+with standard-normal inputs from a seeded generator. One step runs every item forward (x -> y)
+and then inverse (y -> z) through the C ABI's device-pointer entry point on the current torch
+stream. Timing: CUDA events over exactly K steps, barrier + synchronize on both sides, max over
+ranks; each item's buffers are larger than L2 except n = 2^20, which the 1.5 GiB of other traffic
+in a step evicts between its uses.
 
 Printed (rank 0, one JSON line):
-  value       5 n log2(n) batch / t summed over ranks, GFLOP/s (the reference's unit)
-  e2e         the same metric through the drop-in host-pointer call onefft_plan_forward_batched
-              with pinned host buffers: the host->device copy of the inputs and the
-              device->host copy of all outputs are inside the timed region of every step
-  roofline    the transform kernel against the measured HBM copy bandwidth: algorithmic bytes
-              16 n per transform (read 8n + write 8n) / average kernel time
-  cpu_baseline  the reference library (compiled from its own sources) on this host's cores,
-              one shared plan and all cores pulling transforms from an atomic counter
-  detail      single large transforms n = 2^20, 2^24, 2^27 (time, GFLOP/s, GB/s of 16 n)
+  value         sum over items of 2 * 5 n log2(n) batch / step time, GFLOP/s (the reference's
+                unit, 5 n log2 n per transform and direction), summed over ranks
+  e2e           the same metric through the drop-in host-pointer calls (onefft_plan_forward /
+                _inverse for the single transforms, onefft_plan_forward_batched / _inverse for
+                the batch) on pinned host buffers: every step copies all inputs in and all
+                outputs back inside the timed region
+  roofline      the item with the largest share of device time, against the measured HBM copy
+                bandwidth: algorithmic bytes 16 n per transform and direction over its time
+  cpu_baseline  the reference library compiled from its own sources, on this host's cores, on
+                the same workload: one shared plan per size, threads pull transforms (largest
+                first) from an atomic counter and call onefft_plan_forward/_inverse
+  detail        per item: microseconds per direction, GFLOP/s, GB/s of 16 n, passes, launches
 
 With --impl reference only rank 0 runs: it times the reference CPU library on the same workload
-with all host threads and prints the same metric with "impl": "reference".
-Multi-GPU (torchrun, one process per GPU): each rank transforms its own 16384 x 4096 batch
-(weak scaling, no collective on the data path).
+with all host threads and prints the same metric with "impl": "reference". Multi-GPU (torchrun,
+one process per GPU): every rank runs the whole workload on its own data (weak scaling, no
+collective on the data path).
 """
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -40,45 +45,47 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-N_LOG2 = 12
-N = 1 << N_LOG2
-BATCH = 16384
-FLOP_PER_TRANSFORM = 5 * N * N_LOG2
-BYTES_PER_TRANSFORM = 16 * N
-METRIC = "5n*log2(n)/t GFLOP/s, batched FP32 c2c FFT"
-WORKLOAD = {"workload": "batched FP32 complex FFT, 16384 x n=4096, forward, interleaved complex64",
-            "n": N, "batch": BATCH, "direction": "forward", "input": "standard normal re/im (seeded)",
-            "l2": "inputs larger than L2 (512 MiB per buffer), no flush needed"}
+# (name, log2 n, batch)
+ITEMS = [("batch 16384 x 2^12", 12, 16384), ("single 2^20", 20, 1), ("single 2^24", 24, 1), ("single 2^27", 27, 1)]
+METRIC = "5n*log2(n)/t GFLOP/s, FP32 c2c FFT (batched 16384x4096 + single 2^20, 2^24, 2^27; fwd+inv)"
+WORKLOAD = {"workload": "batched FP32 complex FFT: 16384 x n=4096 plus single n=2^20, 2^24, 2^27, "
+                        "forward then inverse each, interleaved complex64 in HBM",
+            "items": [{"n": 1 << l, "batch": b} for _, l, b in ITEMS],
+            "input": "standard normal re/im (seeded torch generator)",
+            "l2": "inputs larger than L2 except n=2^20 (8 MiB), evicted by the other 1.5 GiB of traffic per step"}
+
+
+def flops(log2n: int, batch: int) -> float:
+    return 5.0 * (1 << log2n) * log2n * batch
+
+
+STEP_FLOPS = sum(2 * flops(l, b) for _, l, b in ITEMS)
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-detail", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
 
 def measured_peaks():
-    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
-        with open(path) as f:
-            d = json.load(f)
-        return float(d["hbm_gbs"]), "of measured"
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "of measured"
     except Exception:
         return 6650.0, "of fallback"
 
 
-def ncu_traffic():
-    """DRAM bytes per launch of the transform kernel from the committed ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", "ncu_dram_bytes.json")
+def ncu_traffic(key: str):
+    """DRAM bytes per launch of a kernel from the committed ncu summary, or None."""
     try:
-        with open(path) as f:
-            d = json.load(f)
-        return d.get("k_batched_4096", {}).get("dram_bytes_per_launch")
+        with open(os.path.join(ROOT, "profiles", "ncu_dram_bytes.json")) as f:
+            return json.load(f).get(key)
     except Exception:
         return None
 
@@ -94,15 +101,13 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.lines: list[str] = []
-        self.t = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
                  "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+            threading.Thread(target=self._read, daemon=True).start()
             time.sleep(0.3)
         except Exception:
             self.proc = None
@@ -120,7 +125,7 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, smax, reasons = [], None, set()
+        sm, smax, reasons, power = [], None, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.lines:
             p = [x.strip() for x in line.split(",")]
@@ -129,52 +134,75 @@ class ClockSampler:
             try:
                 sm.append(float(p[1]))
                 smax = float(p[2])
+                power.append(float(p[3]))
             except ValueError:
                 continue
             for nm, v in zip(names, p[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power) if power else None}
 
 
-def cpu_reference_time(x_host: np.ndarray, threads: int, samples: int, kind: str, batch: int = BATCH) -> float:
-    """Seconds for `batch` forward transforms of n=4096 with the CPU library (minimum of samples)."""
+# ---- CPU side: the reference library on the host cores -----------------------------------------
+
+
+def cpu_workload_descriptors():
+    """Descriptors (log2n, complex offset, inverse) of one step, largest transforms first, each
+    direction in its own region (the CPU harness transforms in -> out at the same offset)."""
+    descs = []
+    off = 0
+    for _, l, b in ITEMS:
+        n = 1 << l
+        for inv in (0, 1):
+            for i in range(b):
+                descs.append((l, off + i * n, inv))
+            off += n * b
+    descs.sort(key=lambda d: -d[0])
+    log2n = np.array([d[0] for d in descs], np.int32)
+    offset = np.array([d[1] for d in descs], np.int64)
+    inverse = np.array([d[2] for d in descs], np.int32)
+    return log2n, offset, inverse, off
+
+
+def cpu_step_times(steps: int, warmup: int, samples_per_step: int = 1):
     import oracle
     oracle.build()
-    out = np.empty_like(x_host[:2 * N * batch])
-    t = oracle.cpu_bench_batched(N, batch, threads, False, x_host, out, samples, kind=kind)
-    if t <= 0:
+    kind = "reference" if oracle.have_reference() else "port"
+    cores = oracle.cpu_cores(kind)
+    log2n, offset, inverse, span = cpu_workload_descriptors()
+    rng = np.random.default_rng(12345)
+    x = rng.standard_normal(2 * span, dtype=np.float32)
+    out = np.empty_like(x)
+    for _ in range(warmup):
+        oracle.cpu_bench_uneven(log2n, offset, inverse, cores, x, out, 1, kind=kind)
+    times = [oracle.cpu_bench_uneven(log2n, offset, inverse, cores, x, out, samples_per_step, kind=kind)
+             for _ in range(steps)]
+    if min(times) <= 0:
         raise RuntimeError("CPU reference run failed")
-    return t
+    return times, cores, kind, oracle.cpu_impl(kind)
 
 
 def run_reference(args, rank: int):
     """--impl reference: the reference CPU library on this host, rank 0 only."""
     if rank != 0:
         return
-    import oracle
-    oracle.build()
-    kind = "reference" if oracle.have_reference() else "port"
-    cores = oracle.cpu_cores(kind)
-    rng = np.random.default_rng(12345)
-    x = rng.standard_normal(2 * N * BATCH, dtype=np.float32)
-    out = np.empty_like(x)
-    for _ in range(max(1, args.warmup)):
-        oracle.cpu_bench_batched(N, BATCH, cores, False, x, out, 1, kind=kind)
-    times = []
-    for _ in range(args.steps if args.steps <= 20 else 20):
-        times.append(oracle.cpu_bench_batched(N, BATCH, cores, False, x, out, 1, kind=kind))
+    steps = max(1, min(args.steps, 5))
+    times, cores, kind, impl = cpu_step_times(steps, 1)
     t = sum(times) / len(times)
-    value = FLOP_PER_TRANSFORM * BATCH / t / 1e9
-    line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": len(times),
-            "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
+    value = STEP_FLOPS / t / 1e9
+    sample = (f"the whole step per timed step ({steps} steps after 1 warm-up; {impl} kernels, "
+              f"{cores} threads, largest transforms first)")
+    line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": steps,
+            "warmup": 1, "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
             "config": dict(WORKLOAD, parallelism="host threads"),
-            "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": cores, "kind": kind,
-                             "sample": f"the full 16384 x 4096 forward batch per step ({oracle.cpu_impl(kind)} kernels)"},
+            "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# ---- GPU side ------------------------------------------------------------------------------------
 
 
 def main():
@@ -187,29 +215,51 @@ def main():
         return
 
     import torch
+
     import onefft_b200 as ofb
 
     torch.cuda.set_device(local_rank)
     dist = None
     if world > 1:
         import datetime
+
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
 
     L = ofb.lib()
-    plan = ofb.Plan(N)
-    gen = torch.Generator(device="cuda")
-    gen.manual_seed(1234 + rank)
-    d_in = torch.randn(2 * N * BATCH, device="cuda", generator=gen, dtype=torch.float32)
-    d_out = torch.empty_like(d_in)
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(1234 + rank)
+    work = []
+    for name, l, b in ITEMS:
+        n = 1 << l
+        plan = ofb.Plan(n)
+        x = torch.randn(2 * n * b, device="cuda", generator=gen, dtype=torch.float32)
+        work.append({"name": name, "log2n": l, "batch": b, "plan": plan, "x": x, "y": torch.empty_like(x),
+                     "z": torch.empty_like(x), "passes": plan.passes()})
 
-    def step():
-        rc = L.onefft_dev_forward_batched(plan.handle, d_in.data_ptr(), d_out.data_ptr(), BATCH, sptr)
+    def launch(w, inverse):
+        src, dst = (w["y"], w["z"]) if inverse else (w["x"], w["y"])
+        f = L.onefft_dev_inverse_batched if inverse else L.onefft_dev_forward_batched
+        rc = f(w["plan"].handle, src.data_ptr(), dst.data_ptr(), w["batch"], sptr)
         if rc != 0:
             raise RuntimeError(ofb.last_error())
+
+    nev = 2 * len(work)
+    events = [[torch.cuda.Event(enable_timing=True) for _ in range(nev + 1)] for _ in range(args.steps)]
+
+    def step(ev=None):
+        i = 0
+        for w in work:
+            for inv in (False, True):
+                if ev:
+                    ev[i].record(stream)
+                launch(w, inv)
+                i += 1
+        if ev:
+            ev[i].record(stream)
 
     for _ in range(max(3, args.warmup)):
         step()
@@ -219,101 +269,105 @@ def main():
     clocks = ClockSampler(local_rank)
     clocks.start()
     launches0 = L.onefft_debug_launch_count()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    ev0.record(stream)
-    for _ in range(args.steps):
-        step()
-    ev1.record(stream)
+    for k in range(args.steps):
+        step(events[k])
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     launches = int(L.onefft_debug_launch_count() - launches0)
     clk = clocks.stop()
-    t = ev0.elapsed_time(ev1) / 1e3
+    t = events[0][0].elapsed_time(events[-1][-1]) / 1e3
     if dist:
         tt = torch.tensor([t], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t = tt.item()
     per_step = t / args.steps
-    value = world * FLOP_PER_TRANSFORM * BATCH / per_step / 1e9
+    value = world * STEP_FLOPS / per_step / 1e9
     peak, peak_kind = measured_peaks()
-    achieved = BYTES_PER_TRANSFORM * BATCH / per_step / 1e9  # one kernel launch per step
-    traffic = ncu_traffic()
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_source": peak_kind, "traffic": traffic, "traffic_unit": "bytes per launch",
-                "algorithmic_bytes_per_launch": BYTES_PER_TRANSFORM * BATCH,
-                "frac_of_8TBs_nominal": achieved / 8000.0}
 
-    # ---- end to end through the drop-in host-pointer call (pinned host buffers) ----
-    h_in = torch.empty(2 * N * BATCH, dtype=torch.float32, pin_memory=True)
-    h_out = torch.empty_like(h_in, pin_memory=True)
-    h_in.copy_(d_in.cpu())
-    e2e_steps = max(1, min(args.steps, 10))
-    rc = L.onefft_plan_forward_batched(plan.handle, h_in.data_ptr(), h_out.data_ptr(), BATCH)  # warm-up
-    if rc != 0:
-        raise RuntimeError(ofb.last_error())
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        L.onefft_plan_forward_batched(plan.handle, h_in.data_ptr(), h_out.data_ptr(), BATCH)
-    t_e2e = (time.perf_counter() - t0) / e2e_steps
-    if dist:
-        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = tt.item()
-    torch.cuda.synchronize()
-    ok_e2e = torch.equal(h_out[:2 * N].cuda(), d_out[:2 * N])
-    e2e = {"value": world * FLOP_PER_TRANSFORM * BATCH / t_e2e / 1e9, "unit": "GFLOP/s",
-           "h2d_bytes_per_step": 8 * N * BATCH, "d2h_bytes_per_step": 8 * N * BATCH,
-           "ms_per_step": 1e3 * t_e2e, "steps": e2e_steps, "matches_device_path": bool(ok_e2e),
-           "call": "onefft_plan_forward_batched (pinned host in/out)"}
-    del h_in, h_out
-
-    # ---- single large transforms (same run, reported beside the headline) ----
+    # per item and direction: average launch-group time over the K steps
     detail = {}
-    if not args.no_detail:
-        for lg in (20, 24, 27):
-            n = 1 << lg
-            p = ofb.Plan(n)
-            a = torch.randn(2 * n, device="cuda", generator=gen)
-            b = torch.empty_like(a)
-            flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # 256 MiB > L2
-            reps = 20 if lg < 27 else 5
-            tot = 0.0
-            for r in range(reps + 3):
-                flush.zero_()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                L.onefft_dev_forward_batched(p.handle, a.data_ptr(), b.data_ptr(), 1, sptr)
-                e1.record(stream)
-                torch.cuda.synchronize()
-                if r >= 3:
-                    tot += e0.elapsed_time(e1) / 1e3
-            ts = tot / reps
-            detail[f"n=2^{lg}"] = {"us": 1e6 * ts, "gflops": 5 * n * lg / ts / 1e9, "gbs_16n": 16 * n / ts / 1e9,
-                                   "frac_hbm": 16 * n / ts / 1e9 / peak, "passes": list(p.passes()),
-                                   "l2": "flushed (256 MiB write) before each rep"}
-            p.destroy()
-            del a, b, flush
+    share = []
+    for wi, w in enumerate(work):
+        n, b = 1 << w["log2n"], w["batch"]
+        tt = []
+        for d in range(2):
+            s = sum(events[k][2 * wi + d].elapsed_time(events[k][2 * wi + d + 1]) for k in range(args.steps))
+            tt.append(s / args.steps / 1e3)
+        td = sum(tt) / 2
+        share.append(sum(tt))
+        detail[w["name"]] = {"us_forward": 1e6 * tt[0], "us_inverse": 1e6 * tt[1],
+                             "gflops": flops(w["log2n"], b) / td / 1e9, "gbs_16n": 16 * n * b / td / 1e9,
+                             "frac_hbm": 16 * n * b / td / 1e9 / peak, "passes": list(w["passes"]),
+                             "launches_per_direction": len(w["passes"])}
+    dom = int(np.argmax(share))
+    w = work[dom]
+    n, b = 1 << w["log2n"], w["batch"]
+    td = share[dom] / 2
+    achieved = 16 * n * b / td / 1e9
+    kernel = "k_batched" if len(w["passes"]) == 1 else "k_pass x%d" % len(w["passes"])
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": peak_kind, "kernel": f"{kernel} ({w['name']})",
+                "traffic": ncu_traffic(w["name"]), "traffic_unit": "DRAM bytes per launch (ncu)",
+                "algorithmic_bytes_per_launch": 16 * n * b / len(w["passes"]),
+                "share_of_step": share[dom] / sum(share), "frac_of_8TBs_nominal": achieved / 8000.0}
+
+    # ---- end to end through the drop-in host-pointer calls (pinned host buffers) ----
+    e2e = None
+    if not args.no_e2e:
+        host = []
+        for w in work:
+            hx = torch.empty(w["x"].numel(), dtype=torch.float32, pin_memory=True)
+            hx.copy_(w["x"])
+            host.append((w, hx, torch.empty_like(hx, pin_memory=True), torch.empty_like(hx, pin_memory=True)))
+
+        def e2e_step():
+            for w, hx, hy, hz in host:
+                h = w["plan"].handle
+                if w["batch"] > 1:
+                    rc = L.onefft_plan_forward_batched(h, hx.data_ptr(), hy.data_ptr(), w["batch"])
+                    rc |= L.onefft_plan_inverse_batched(h, hy.data_ptr(), hz.data_ptr(), w["batch"])
+                    if rc:
+                        raise RuntimeError(ofb.last_error())
+                else:
+                    L.onefft_plan_forward(h, hx.data_ptr(), hy.data_ptr())
+                    L.onefft_plan_inverse(h, hy.data_ptr(), hz.data_ptr())
+
+        e2e_step()
+        e2e_steps = max(1, min(args.steps, 5))
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            e2e_step()
+        t_e2e = (time.perf_counter() - t0) / e2e_steps
+        if dist:
+            tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t_e2e = tt.item()
+        same = all(torch.equal(hy[:4096].cuda(), w["y"][:4096]) for w, hx, hy, hz in host)
+        nbytes = sum(2 * 8 * (1 << w["log2n"]) * w["batch"] for w in work)
+        e2e = {"value": world * STEP_FLOPS / t_e2e / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "ms_per_step": 1e3 * t_e2e, "steps": e2e_steps,
+               "matches_device_path": bool(same),
+               "calls": "onefft_plan_forward/_inverse (single) and onefft_plan_forward/_inverse_batched (batch), "
+                        "pinned host buffers"}
+        del host
 
     # ---- CPU baseline: the reference library on this host (rank 0, N = 1) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            import oracle
-            oracle.build()
-            kind = "reference" if oracle.have_reference() else "port"
-            cores = oracle.cpu_cores(kind)
-            xh = d_in.cpu().numpy()
-            tc = cpu_reference_time(xh, cores, 5, kind)
-            cpu = {"value": FLOP_PER_TRANSFORM * BATCH / tc / 1e9, "unit": "GFLOP/s", "cores": cores, "kind": kind,
-                   "sample": f"full 16384 x 4096 forward batch, min of 5 passes, {oracle.cpu_impl(kind)} kernels",
-                   "ms_per_step": 1e3 * tc}
+            times, cores, kind, impl = cpu_step_times(3, 1)
+            tc = min(times)
+            cpu = {"value": STEP_FLOPS / tc / 1e9, "unit": "GFLOP/s", "cores": cores, "kind": kind,
+                   "ms_per_step": 1e3 * tc,
+                   "sample": f"the whole step (all items, both directions), min of 3 runs after 1 warm-up; "
+                             f"{impl} kernels, {cores} threads, largest transforms first"}
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "unit": "GFLOP/s", "cores": None, "kind": None, "sample": f"failed: {e}"}
 
@@ -321,11 +375,12 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
                 "warmup": max(3, args.warmup), "ms_per_step": 1e3 * per_step, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": dict(WORKLOAD, parallelism=f"dp{world} (independent batches per GPU)"),
+                "config": dict(WORKLOAD, parallelism=f"dp{world} (independent work per GPU, no collective)"),
                 "impl": "ours", "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
                 "gpu_launches": launches, "detail": detail}
         print(json.dumps(line), flush=True)
-    plan.destroy()
+    for w in work:
+        w["plan"].destroy()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -60,6 +60,15 @@ ONEFFT_API int onefft_plan_inverse_batched(const onefft_plan *plan, const float 
  * tests that exercise every pass kernel at small sizes. NULL on an invalid split. */
 ONEFFT_API onefft_plan *onefft_plan_create_split(size_t n, int npass, const int *log2_len);
 
+/* As onefft_plan_create_split, also choosing each pass's tile width: 2^log2_cols[p] adjacent
+ * columns per thread block (2 .. 4, at most 16384 values per tile; NULL = default widths),
+ * whether the array between passes is stored with L2 evict-last priority (l2_keep != 0), and,
+ * for three passes, log2_chunk > 0 to run the first two passes chunk by chunk over 2^log2_chunk
+ * columns of the last digit so that each chunk's intermediate values stay in L2 (0 = whole
+ * passes). */
+ONEFFT_API onefft_plan *onefft_plan_create_tiles(size_t n, int npass, const int *log2_len, const int *log2_cols,
+                                                 int l2_keep, int log2_chunk);
+
 /* Number of passes of a plan and their log2 lengths (up to 3 are written to log2_len). */
 ONEFFT_API int onefft_plan_passes(const onefft_plan *plan, int *log2_len);
 

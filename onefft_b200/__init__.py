@@ -31,7 +31,7 @@ C_SYMBOLS = (
     "onefft_plan_size", "onefft_implementation",
     "onefft_dev_forward_batched", "onefft_dev_inverse_batched", "onefft_dev_adjoint_batched",
     "onefft_plan_forward_batched", "onefft_plan_inverse_batched",
-    "onefft_plan_create_split", "onefft_plan_passes",
+    "onefft_plan_create_split", "onefft_plan_create_tiles", "onefft_plan_passes",
     "onefft_last_error", "onefft_debug_fail_alloc", "onefft_debug_twiddles", "onefft_debug_launch_count",
 )
 
@@ -59,6 +59,9 @@ def lib() -> ctypes.CDLL:
     L.onefft_plan_create.restype = _vp
     L.onefft_plan_create_split.argtypes = [_sz, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.onefft_plan_create_split.restype = _vp
+    L.onefft_plan_create_tiles.argtypes = [_sz, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                           ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int]
+    L.onefft_plan_create_tiles.restype = _vp
     L.onefft_plan_destroy.argtypes = [_vp]
     L.onefft_plan_destroy.restype = None
     L.onefft_plan_forward.argtypes = [_vp, _vp, _vp]
@@ -150,13 +153,17 @@ def cache_clear() -> None:
 class Plan:
     """Owns the device tables of one size (OneFFT's onefft::Plan, include/onefft.h:136-167)."""
 
-    def __init__(self, n: int, split: tuple[int, ...] | None = None):
+    def __init__(self, n: int, split: tuple[int, ...] | None = None, cols: tuple[int, ...] | None = None,
+                 l2_keep: bool = True, chunk: int = 0):
+        """split: log2 pass lengths (None = tuned table); cols: log2 tile widths per pass;
+        chunk: three passes only, log2 last-digit columns per L2-resident chunk (0 = none)."""
         L = lib()
         if split is None:
             h = L.onefft_plan_create(n)
         else:
             arr = (ctypes.c_int * len(split))(*split)
-            h = L.onefft_plan_create_split(n, len(split), arr)
+            carr = (ctypes.c_int * len(split))(*cols) if cols is not None else None
+            h = L.onefft_plan_create_tiles(n, len(split), arr, carr, int(l2_keep), int(chunk))
         if not h:
             raise ValueError(f"no plan for n={n}: {last_error()}")
         self._h = h

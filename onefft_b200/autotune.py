@@ -1,0 +1,131 @@
+"""Autotuner of the pass split and tile widths per transform size.
+
+    python -m onefft_b200.autotune [--min 15] [--max 27] [--out tuned.json]
+
+For every log2 n in range it enumerates candidate shapes — two or three passes with lengths
+2^4 .. 2^12, tile widths of 4, 8 or 16 columns per block, L2 evict-last stores on or off — builds
+each as a plan (onefft_plan_create_tiles), checks its forward result against the default plan,
+times the forward transform with CUDA events (L2 flushed before every repetition), and prints
+the fastest shape per size as the C table used by onefft_api.cu (tuned_shape) plus a JSON record.
+"""
+from __future__ import annotations
+
+import argparse
+import itertools
+import json
+import sys
+
+import torch
+
+import onefft_b200 as ofb
+
+
+def tile_ok(l: int, c: int) -> bool:
+    return 4 <= l <= 12 and c <= 4 and l + c <= 14 and (c >= 2 or (c == 1 and l >= 10))
+
+
+def candidates(m: int):
+    """(log2 lengths, log2 tile widths, log2 chunk) shapes worth timing for 2^m."""
+    out = []
+    # two passes
+    for l0 in range(4, 13):
+        l1 = m - l0
+        if 4 <= l1 <= 12:
+            for c0 in (1, 2, 3, 4):
+                for c1 in (1, 2, 3, 4):
+                    if tile_ok(l0, c0) and tile_ok(l1, c1) and l0 + c0 >= 11 and l1 + c1 >= 11:
+                        out.append(((l0, l1), (c0, c1), 0))
+    # three passes, balanced lengths; passes 0+1 whole or in L2-sized chunks of the last digit
+    for ls in itertools.product(range(5, 13), repeat=3):
+        if sum(ls) != m or max(ls) - min(ls) > 3:
+            continue
+        for cs in itertools.product((2, 3, 4), repeat=3):
+            if all(tile_ok(l, c) and l + c >= 11 for l, c in zip(ls, cs)) and cs[0] <= ls[2]:
+                out.append((ls, cs, 0))
+                for mib in (16, 32, 64):
+                    g = (mib << 20).bit_length() - 1 - 3 - ls[0] - ls[1]  # 8 bytes per value
+                    if cs[0] <= g < ls[2]:
+                        out.append((ls, cs, g))
+    return out
+
+
+def time_plan(plan, x, y, reps: int, flush) -> float:
+    stream = torch.cuda.current_stream()
+    ts = []
+    for r in range(reps + 2):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plan.dev_forward(x.data_ptr(), y.data_ptr(), 1, stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if r >= 2:
+            ts.append(e0.elapsed_time(e1) * 1e3)
+    ts.sort()
+    return ts[len(ts) // 2]
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--min", type=int, default=15)
+    ap.add_argument("--max", type=int, default=27)
+    ap.add_argument("--reps", type=int, default=7)
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--max-candidates", type=int, default=1000)
+    args = ap.parse_args()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    results = {}
+    for m in range(args.min, args.max + 1):
+        n = 1 << m
+        x = torch.randn(2 * n, device="cuda")
+        y = torch.empty_like(x)
+        ref = ofb.Plan(n)
+        ref.dev_forward(x.data_ptr(), y.data_ptr())
+        torch.cuda.synchronize()
+        want = y.clone()
+        scale = want.abs().max().item()
+        best = None
+        rows = []
+        cands = candidates(m)[: args.max_candidates]
+        for ls, cs, g in cands:
+            for keep in (True, False):
+                try:
+                    p = ofb.Plan(n, split=ls, cols=cs, l2_keep=keep, chunk=g)
+                except ValueError:
+                    continue
+                y.zero_()
+                p.dev_forward(x.data_ptr(), y.data_ptr())
+                torch.cuda.synchronize()
+                err = (y - want).abs().max().item() / scale
+                if err > 1e-5:
+                    print(f"m={m} {ls} {cs} chunk={g} keep={keep}: result differs ({err:.2e}), skipped",
+                          file=sys.stderr)
+                    p.destroy()
+                    continue
+                us = time_plan(p, x, y, args.reps, flush)
+                p.destroy()
+                rows.append({"len": ls, "cols": cs, "l2_keep": keep, "chunk": g, "us": us,
+                             "gbs_16n": 16 * n / us / 1e3})
+                if best is None or us < best["us"]:
+                    best = rows[-1]
+        base_us = time_plan(ref, x, y, args.reps, flush)
+        ref.destroy()
+        results[m] = {"best": best, "default_us": base_us, "all": sorted(rows, key=lambda r: r["us"])[:10]}
+        print(f"m={m}: best {best['len']} cols {best['cols']} chunk {best['chunk']} keep={best['l2_keep']} "
+              f"{best['us']:.1f} us ({best['gbs_16n']:.0f} GB/s of 16n); default {base_us:.1f} us", flush=True)
+        del x, y, want
+        torch.cuda.empty_cache()
+    print("// tuned shapes: {npass, {len}, {cols}, l2_keep, chunk} for log2 n =", args.min, "..", args.max)
+    for m, r in results.items():
+        b = r["best"]
+        ls = list(b["len"]) + [0] * (3 - len(b["len"]))
+        cs = list(b["cols"]) + [0] * (3 - len(b["cols"]))
+        print(f"    /* {m} */ {{{len(b['len'])}, {{{ls[0]}, {ls[1]}, {ls[2]}}}, {{{cs[0]}, {cs[1]}, {cs[2]}}}, "
+              f"{int(b['l2_keep'])}, {b['chunk']}}},")
+    if args.out:
+        with open(args.out, "w") as f:
+            json.dump(results, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -216,28 +216,38 @@ __device__ __forceinline__ int stage_out_index(int b, int p) {
     return ((b >> LNS) << (LR + LNS)) + (b & ((1 << LNS) - 1)) + (p << LNS);
 }
 
-// Shared-memory slot of complex index x of a tile: one pad slot every 16 entries keeps the
-// stride-16 writes of the first stage and the column-interleaved layouts free of bank conflicts
-// for 8-byte accesses.
+// Shared-memory slot of linear tile index x: one pad slot every 16 entries keeps the stride-16
+// writes of the first stage and the column-interleaved layouts free of bank conflicts for 8-byte
+// accesses.
 __device__ __forceinline__ int spad(int x) { return x + (x >> 4); }
+// Padded size of a compile-time displacement D. Every access below is spad(x0) + padc(D) with a
+// per-thread base x0 and a compile-time D such that (x0 mod 16) + (D mod 16) < 16, which makes
+// spad(x0 + D) == spad(x0) + padc(D): the address is one register plus an immediate.
+__host__ __device__ constexpr int padc(int d) { return d + (d >> 4); }
 
 // Runs every stage of one column's FFT. On entry v[k] = X[j + T k]; on exit v[k] = Y[j + T k].
-// SIdx maps a column-local element index to the shared-memory slot of this thread's column.
+// The column's element e lives at linear tile index e * LM + cofs: LM = C, cofs = c for the
+// column-interleaved layout ([e][c], C columns), LM = 1, cofs = c L for whole columns ([c][e]).
 // All threads of the block must call this (it synchronises).
-template <int LOG_L, int S = 0, class SIdx>
+template <int LOG_L, int LM, int S = 0>
 __device__ __forceinline__ void tile_fft(float2 (&v)[16], int j, const float2* __restrict__ stw, float2* smem,
-                                         const SIdx& sidx) {
+                                         int cofs) {
     using St = Stages<LOG_L>;
     stage_compute<LOG_L, S>(v, j, stw);
     if constexpr (S + 1 < St::COUNT) {
-        // intermediate stages are radix 16: one butterfly per thread, b = j
+        // intermediate stages are radix 16: one butterfly per thread, b = j, output p at
+        // E0 + p Ns with E0 = (j / Ns) 16 Ns + (j mod Ns)
+        constexpr int LNS = St::log2_ns(S);
+        constexpr int NS = 1 << LNS;
+        float2* w = smem + spad((((j >> LNS) << (4 + LNS)) + (j & (NS - 1))) * LM + cofs);
 #pragma unroll
-        for (int p = 0; p < 16; ++p) smem[sidx(stage_out_index<LOG_L, S>(j, p))] = v[p];
+        for (int p = 0; p < 16; ++p) w[padc(p * NS * LM)] = v[p];
         __syncthreads();
+        const float2* r = smem + spad(j * LM + cofs);
 #pragma unroll
-        for (int k = 0; k < 16; ++k) v[k] = smem[sidx(j + St::T * k)];
+        for (int k = 0; k < 16; ++k) v[k] = r[padc(k * St::T * LM)];
         __syncthreads();
-        tile_fft<LOG_L, S + 1>(v, j, stw, smem, sidx);
+        tile_fft<LOG_L, LM, S + 1>(v, j, stw, smem, cofs);
     }
 }
 

@@ -54,12 +54,27 @@ __global__ void k_big_table(double2* __restrict__ lo, double2* __restrict__ hi, 
         hi[idx - nlo] = root_f64((unsigned long long)(idx - nlo) << lo_bits, (unsigned)log2n);
 }
 
-// w_n^t for t < n from the two-level tables: FP64 product, rounded once to FP32.
-__device__ __forceinline__ float2 big_twiddle(const double2* __restrict__ lo, const double2* __restrict__ hi,
-                                              int lo_bits, unsigned t) {
-    double2 a = __ldg(lo + (t & ((1u << lo_bits) - 1)));
-    double2 b = __ldg(hi + (t >> lo_bits));
-    return make_float2((float)fma(a.x, b.x, -a.y * b.y), (float)fma(a.x, b.y, a.y * b.x));
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+
+// w_n^t for t < n from the two-level tables, in FP64.
+__device__ __forceinline__ double2 big_twiddle_f64(const double2* __restrict__ lo, const double2* __restrict__ hi,
+                                                   int lo_bits, unsigned t) {
+    return zmul(__ldg(lo + (t & ((1u << lo_bits) - 1))), __ldg(hi + (t >> lo_bits)));
+}
+
+// L2 cache hints: the input of a transform is read exactly once (evict first); the intermediate
+// array between passes should stay in L2 for the next pass (evict last).
+__device__ __forceinline__ float2 ld_stream(const float2* p) { return __ldcs(p); }
+__device__ __forceinline__ unsigned long long policy_evict_last() {
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ void st_policy(float2* p, float2 v, unsigned long long pol) {
+    asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(p), "f"(v.x), "f"(v.y), "l"(pol)
+                 : "memory");
 }
 
 // ---- n <= 8 --------------------------------------------------------------------------------------
@@ -94,19 +109,18 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4))
     const int c = tid >> (LOG_L - 4);
     const long long g = (long long)blockIdx.x * C + c;
     const bool active = g < batch;
-    const float2* src = in + g * L;
-    float2* dst = out + g * L;
+    const float2* src = in + g * L + j;
+    float2* dst = out + g * L + j;
     float2 v[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-        float2 x = active ? __ldg(src + j + T * k) : make_float2(0.f, 0.f);
+        float2 x = active ? ld_stream(src + T * k) : make_float2(0.f, 0.f);
         v[k] = inverse ? swap_ri(x) : x;
     }
-    auto sidx = [c](int e) { return spad(c * L + e); };
-    tile_fft<LOG_L>(v, j, stw, smem, sidx);
+    tile_fft<LOG_L, 1>(v, j, stw, smem, c << LOG_L);
     if (active) {
 #pragma unroll
-        for (int k = 0; k < 16; ++k) dst[j + T * k] = inverse ? swap_ri(v[k]) : v[k];
+        for (int k = 0; k < 16; ++k) dst[T * k] = inverse ? swap_ri(v[k]) : v[k];
     }
 }
 
@@ -117,17 +131,17 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4))
 // MODE 2: last pass, in place on out, no twiddle.
 template <int LOG_L, int LOG_C, int MODE>
 __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4)) k_pass(PassArgs a) {
-    constexpr int L = 1 << LOG_L, T = L / 16, C = 1 << LOG_C, THREADS = C * T;
+    constexpr int L = 1 << LOG_L, T = L / 16, C = 1 << LOG_C;
     extern __shared__ float2 smem[];
     const int tid = threadIdx.x;
     const int c = tid & (C - 1);
     const int j = tid >> LOG_C;
     const long long tstride = 1ll << a.log2n;  // batch stride between transforms
-    const float2* src = a.in + (long long)blockIdx.y * tstride;
-    float2* dst = a.out + (long long)blockIdx.y * tstride;
-    const unsigned col0 = blockIdx.x * C;
-    float2 v[16];
-    unsigned base;  // element (e) of this thread's column is at base + (e << a.log_s)
+    const unsigned t = blockIdx.x;
+    const unsigned col0 = a.tli >= 31 ? (t << LOG_C)
+                                      : ((a.outer_base + (t >> a.tli)) << a.outer_shift) + a.inner_base +
+                                            ((t & ((1u << a.tli) - 1)) << LOG_C);
+    unsigned base;  // element e of this thread's column is at base + (e << a.log_s)
     if (MODE == 0) {
         base = col0 + c;
     } else {
@@ -135,49 +149,74 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4)) k_pass(PassArgs a) {
         unsigned h = col0 >> a.log_s;
         base = q + (h << (a.log_s + LOG_L));
     }
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        // passes after the first read and write `out` in place: the read-only cache path is
-        // only used where the kernel never writes what it reads
-        const float2* p = src + base + ((unsigned)(j + T * k) << a.log_s);
-        float2 x = MODE == 0 ? __ldg(p) : *p;
-        v[k] = a.swap_in ? swap_ri(x) : x;
+    // Inter-pass twiddles w_n^(F (j + T kk)) for this thread's outputs, F = r (first pass,
+    // per column) or S h (middle pass, per block), split as w^(F j) * w^(F T kk): the 16 factors
+    // w^(F T kk) of each column are evaluated once per block from the FP64 tables into shared
+    // memory (rows padded to 17 so the columns of a warp hit distinct banks), w^(F j) once per
+    // thread; each is rounded once to FP32 and their product applied in FP32.
+    float2* tws = smem + spad(C * L - 1) + 1;
+    if (MODE != 2) {
+        const unsigned hs = (col0 >> a.log_s) << a.log_s;
+        for (int i = tid; i < (MODE == 0 ? C : 1) * 16; i += C * T) {
+            const int cc = i >> 4, kk = i & 15;
+            const unsigned f = MODE == 0 ? col0 + cc : hs;
+            double2 w = big_twiddle_f64(a.tw_lo, a.tw_hi, a.lo_bits, f * (unsigned)T * (unsigned)kk);
+            tws[cc * 17 + kk] = make_float2((float)w.x, (float)w.y);
+        }
     }
-    auto sidx = [c](int e) { return spad(e * C + c); };
-    tile_fft<LOG_L>(v, j, a.stw, smem, sidx);
+    // element j + T k of the column: p0 + k * estep
+    const long long estep = (long long)T << a.log_s;
+    const long long off0 = (long long)blockIdx.y * tstride + base + ((long long)j << a.log_s);
+    float2 v[16];
+    {
+        const float2* p0 = a.in + off0;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            // The first pass streams the input, which is never read again. Later passes read
+            // and write `out` in place, so they avoid the read-only cache path.
+            float2 x = MODE == 0 ? ld_stream(p0 + k * estep) : p0[k * estep];
+            v[k] = a.swap_in ? swap_ri(x) : x;
+        }
+    }
+    tile_fft<LOG_L, C>(v, j, a.stw, smem, c);
+    if (MODE != 2) {
+        if (Stages<LOG_L>::COUNT == 1) __syncthreads();  // tile_fft had no barrier to publish tws
+        const unsigned f = MODE == 0 ? col0 + c : (col0 >> a.log_s) << a.log_s;
+        const double2 wj = big_twiddle_f64(a.tw_lo, a.tw_hi, a.lo_bits, f * (unsigned)j);
+        const float2 wjf = make_float2((float)wj.x, (float)wj.y);
+        const float2* tw = tws + (MODE == 0 ? c * 17 : 0);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[k] = cmul(v[k], cmul(wjf, tw[k]));
+    }
+    const unsigned long long keep = a.l2_keep ? policy_evict_last() : 0ull;
     if (MODE == 0) {
-        const unsigned r = col0 + c;
+        // Transpose through shared memory so that each column's L results leave as one
+        // contiguous, coalesced run: thread t then stores values kk0 + T i (i = 0..15) of
+        // column cc = t / T, at its digit-reversed place.
+        {
+            float2* w = smem + spad(j * C + c);
 #pragma unroll
-        for (int k = 0; k < 16; ++k)
-            v[k] = cmul(v[k], big_twiddle(a.tw_lo, a.tw_hi, a.lo_bits, r * (unsigned)(j + T * k)));
-        // transpose through shared memory so that each column's L results leave as one
-        // contiguous, coalesced run
-#pragma unroll
-        for (int k = 0; k < 16; ++k) smem[spad((j + T * k) * C + c)] = v[k];
+            for (int k = 0; k < 16; ++k) w[padc(k * T * C)] = v[k];
+        }
         __syncthreads();
+        const int cc = tid >> (LOG_L - 4), kk0 = tid & (T - 1);
+        const unsigned rr = col0 + cc;
+        const unsigned j2 = rr & ((1u << a.rev_b2) - 1), j1 = rr >> a.rev_b2;
+        float2* q = a.out + (long long)blockIdx.y * tstride + (((j1 + (j2 << a.rev_b1)) << LOG_L) + kk0);
+        const float2* r = smem + spad(kk0 * C + cc);
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
-            int o = tid + THREADS * i;
-            int cc = o >> LOG_L, kk = o & (L - 1);
-            unsigned rr = col0 + cc;
-            unsigned j2 = rr & ((1u << a.rev_b2) - 1), j1 = rr >> a.rev_b2;
-            unsigned pos = ((j1 + (j2 << a.rev_b1)) << LOG_L) + kk;
-            float2 x = smem[spad(kk * C + cc)];
-            dst[pos] = a.swap_out ? swap_ri(x) : x;
+            float2 x = r[padc(i * T * C)];
+            if (a.l2_keep) st_policy(q + i * T, x, keep);
+            else q[i * T] = x;
         }
     } else {
-        if (MODE == 1) {
-            const unsigned h = col0 >> a.log_s;
-            const unsigned mask = (1u << a.log2n) - 1;
-#pragma unroll
-            for (int k = 0; k < 16; ++k)
-                v[k] = cmul(v[k], big_twiddle(a.tw_lo, a.tw_hi, a.lo_bits,
-                                              ((h * (unsigned)(j + T * k)) << a.log_s) & mask));
-        }
+        float2* p0 = a.out + off0;
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
             float2 x = a.swap_out ? swap_ri(v[k]) : v[k];
-            dst[base + ((unsigned)(j + T * k) << a.log_s)] = x;
+            if (MODE == 1 && a.l2_keep) st_policy(p0 + k * estep, x, keep);
+            else p0[k * estep] = x;
         }
     }
 }
@@ -257,22 +296,30 @@ cudaError_t launch_single_kernel(int log2n, const float2* in, float2* out, long 
     }
 }
 
-// Tile width (columns per block) of a pass of length 2^log_l: 16 columns (one 128-byte line per
-// row) up to 256 points, then 8 and 4 so the tile stays within 16384 values (136 KiB of shared
-// memory with padding at 4 x 4096).
-int pass_log_c(int log_l) { return log_l <= 8 ? 4 : log_l == 9 ? 3 : 2; }
+// Default tile width (columns per block) of a pass of length 2^log_l: 16 columns (one 128-byte
+// line per row) up to 512 points, then 8 at 1024 and 4 beyond, so a tile holds at most 16384
+// values (136 KiB of shared memory with padding at 4 x 4096).
+int pass_log_c(int log_l) { return log_l <= 9 ? 4 : log_l == 10 ? 3 : 2; }
 
-template <int LOG_L, int MODE>
+// Tile widths compiled for each pass length: 2^2 .. 2^4 columns with at most 16384 values, and
+// 2 columns for lengths 2^10 .. 2^12 (two tiles of adjacent blocks then share each 32-byte
+// sector of a row).
+bool pass_tile_supported(int log_l, int log_c) {
+    return log_l >= 4 && log_l <= 12 && log_c <= 4 && log_l + log_c <= 14 && (log_c >= 2 || (log_c == 1 && log_l >= 10));
+}
+
+template <int LOG_L, int LOG_C, int MODE>
 static cudaError_t launch_pass_t(const PassArgs& a, int batch, cudaStream_t stream) {
-    constexpr int LOG_C = LOG_L <= 8 ? 4 : LOG_L == 9 ? 3 : 2;
     constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
-    constexpr int SMEM = smem_bytes(LOG_L, LOG_C);
+    // the tile, then the inter-pass twiddle factors (17 per column)
+    constexpr int SMEM = smem_bytes(LOG_L, LOG_C) + (MODE == 2 ? 0 : (int)sizeof(float2) * 17 * (1 << LOG_C));
     auto kernel = k_pass<LOG_L, LOG_C, MODE>;
     static cudaError_t attr = set_smem(kernel, SMEM);
     if (attr != cudaSuccess) return attr;
     unsigned cols = 1u << (a.log2n - LOG_L);
-    dim3 grid(cols >> LOG_C, 1, 1);
+    dim3 grid(a.ntiles ? a.ntiles : cols >> LOG_C, 1, 1);
     PassArgs b = a;
+    if (!a.ntiles) b.tli = 31;
     while (batch > 0) {
         int now = batch < 65535 ? batch : 65535;
         grid.y = (unsigned)now;
@@ -284,27 +331,43 @@ static cudaError_t launch_pass_t(const PassArgs& a, int batch, cudaStream_t stre
     return cudaGetLastError();
 }
 
+template <int LOG_L, int MODE>
+static cudaError_t launch_pass_c(int log_c, const PassArgs& a, int batch, cudaStream_t stream) {
+    if constexpr (LOG_L >= 10) {
+        if (log_c == 1) return launch_pass_t<LOG_L, 1, MODE>(a, batch, stream);
+    }
+    if (log_c == 2) return launch_pass_t<LOG_L, 2, MODE>(a, batch, stream);
+    if constexpr (LOG_L + 3 <= 14) {
+        if (log_c == 3) return launch_pass_t<LOG_L, 3, MODE>(a, batch, stream);
+    }
+    if constexpr (LOG_L + 4 <= 14) {
+        if (log_c == 4) return launch_pass_t<LOG_L, 4, MODE>(a, batch, stream);
+    }
+    return cudaErrorInvalidValue;
+}
+
 template <int MODE>
-static cudaError_t launch_pass_mode(int log_l, const PassArgs& a, int batch, cudaStream_t stream) {
+static cudaError_t launch_pass_mode(int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t stream) {
     switch (log_l) {
-    case 4: return launch_pass_t<4, MODE>(a, batch, stream);
-    case 5: return launch_pass_t<5, MODE>(a, batch, stream);
-    case 6: return launch_pass_t<6, MODE>(a, batch, stream);
-    case 7: return launch_pass_t<7, MODE>(a, batch, stream);
-    case 8: return launch_pass_t<8, MODE>(a, batch, stream);
-    case 9: return launch_pass_t<9, MODE>(a, batch, stream);
-    case 10: return launch_pass_t<10, MODE>(a, batch, stream);
-    case 11: return launch_pass_t<11, MODE>(a, batch, stream);
-    case 12: return launch_pass_t<12, MODE>(a, batch, stream);
+    case 4: return launch_pass_c<4, MODE>(log_c, a, batch, stream);
+    case 5: return launch_pass_c<5, MODE>(log_c, a, batch, stream);
+    case 6: return launch_pass_c<6, MODE>(log_c, a, batch, stream);
+    case 7: return launch_pass_c<7, MODE>(log_c, a, batch, stream);
+    case 8: return launch_pass_c<8, MODE>(log_c, a, batch, stream);
+    case 9: return launch_pass_c<9, MODE>(log_c, a, batch, stream);
+    case 10: return launch_pass_c<10, MODE>(log_c, a, batch, stream);
+    case 11: return launch_pass_c<11, MODE>(log_c, a, batch, stream);
+    case 12: return launch_pass_c<12, MODE>(log_c, a, batch, stream);
     default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t launch_pass(int mode, int log_l, const PassArgs& a, int batch, cudaStream_t stream) {
+cudaError_t launch_pass(int mode, int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t stream) {
+    if (!pass_tile_supported(log_l, log_c)) return cudaErrorInvalidValue;
     switch (mode) {
-    case 0: return launch_pass_mode<0>(log_l, a, batch, stream);
-    case 1: return launch_pass_mode<1>(log_l, a, batch, stream);
-    default: return launch_pass_mode<2>(log_l, a, batch, stream);
+    case 0: return launch_pass_mode<0>(log_l, log_c, a, batch, stream);
+    case 1: return launch_pass_mode<1>(log_l, log_c, a, batch, stream);
+    default: return launch_pass_mode<2>(log_l, log_c, a, batch, stream);
     }
 }
 

@@ -20,6 +20,15 @@ struct PassArgs {
     const double2* tw_lo;   // two-level FP64 tables of w_n
     const double2* tw_hi;
     int lo_bits;
+    int l2_keep;     // store the intermediate array with L2 evict-last priority
+    // Tile t of a launch starts at column
+    //   col0 = ((outer_base + (t >> tli)) << outer_shift) + inner_base + ((t mod 2^tli) << log_c)
+    // which lets a launch cover one chunk of the columns (tli = 31: col0 = t << log_c).
+    int tli;
+    int outer_shift;
+    unsigned outer_base;
+    unsigned inner_base;
+    unsigned ntiles;  // grid size of the launch (tiles per transform)
 };
 
 // Largest size handled by one kernel (k_tiny / k_batched).
@@ -27,10 +36,11 @@ constexpr int kMaxSingleLog2 = 14;
 
 int batched_log_c(int log_l);
 int pass_log_c(int log_l);
+bool pass_tile_supported(int log_l, int log_c);
 
 cudaError_t launch_single_kernel(int log2n, const float2* in, float2* out, long long batch, const float2* stw,
                                  int inverse, cudaStream_t stream);
-cudaError_t launch_pass(int mode, int log_l, const PassArgs& a, int batch, cudaStream_t stream);
+cudaError_t launch_pass(int mode, int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t stream);
 cudaError_t launch_stage_table(float2* dst, int log_l, cudaStream_t stream);
 cudaError_t launch_big_table(double2* lo, double2* hi, int log2n, int lo_bits, cudaStream_t stream);
 int stage_table_entries_host(int log_l);

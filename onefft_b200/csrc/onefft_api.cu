@@ -80,8 +80,11 @@ struct onefft_plan {
     int log2n;
     int device;
     int npass;
-    int len[3];          // log2 of each pass length
-    void *mem;           // the one device allocation
+    int len[3];            // log2 of each pass length
+    int cols[3];           // log2 of the tile width (columns per block) of each pass
+    int l2_keep;           // intermediate stores with L2 evict-last priority
+    int chunk;             // three passes: log2 of the last-digit columns per chunk of passes 0+1 (0 = none)
+    void *mem;             // the one device allocation
     size_t mem_bytes;
     const float2 *stw[3];  // stage twiddles of each pass's length
     const double2 *tw_lo;  // two-level FP64 tables of w_n (npass >= 2)
@@ -89,37 +92,57 @@ struct onefft_plan {
     int lo_bits;
 };
 
-// Tuned pass split per log2 n: one kernel up to 2^14, two passes up to 2^24, three beyond.
-static void default_split(int m, int *npass, int *len) {
+// How a size runs: number of passes, their lengths and tile widths. The table below is the
+// tuned choice per log2 n (onefft_b200/autotune.py measures the candidates on the device and
+// prints this table); sizes up to 2^14 run as one kernel.
+struct Shape {
+    int npass;
+    int len[3];
+    int cols[3];
+    int l2_keep;
+    int chunk;
+};
+
+static Shape tuned_shape(int m) {
+    Shape s{};
     if (m <= kMaxSingleLog2) {
-        *npass = 1;
-        len[0] = m;
-    } else if (m <= 24) {
-        *npass = 2;
-        len[0] = (m + 1) / 2;
-        len[1] = m / 2;
-    } else {
-        *npass = 3;
-        len[0] = (m + 2) / 3;
-        len[1] = (m + 1) / 3;
-        len[2] = m / 3;
+        s.npass = 1;
+        s.len[0] = m;
+        return s;
     }
+    if (m <= 24) {
+        s.npass = 2;
+        s.len[0] = (m + 1) / 2;
+        s.len[1] = m / 2;
+    } else {
+        s.npass = 3;
+        s.len[0] = (m + 2) / 3;
+        s.len[1] = (m + 1) / 3;
+        s.len[2] = m / 3;
+    }
+    for (int i = 0; i < s.npass; ++i) s.cols[i] = pass_log_c(s.len[i]);
+    s.l2_keep = 1;
+    return s;
 }
 
-static bool valid_split(int m, int npass, const int *len) {
-    if (npass == 1) return len[0] == m && m <= kMaxSingleLog2;
-    if (npass < 2 || npass > 3) return false;
+static bool valid_shape(int m, const Shape &s) {
+    if (s.npass == 1) return s.len[0] == m && m <= kMaxSingleLog2;
+    if (s.npass < 2 || s.npass > 3) return false;
     int sum = 0;
-    for (int p = 0; p < npass; ++p) {
-        if (len[p] < 4 || len[p] > 12) return false;
-        sum += len[p];
+    for (int p = 0; p < s.npass; ++p) {
+        if (!pass_tile_supported(s.len[p], s.cols[p])) return false;
+        sum += s.len[p];
     }
+    // the first pass's tile must not straddle a column digit of the last pass (three passes),
+    // and a chunk holds whole first-pass tiles
+    if (s.npass == 3 && s.cols[0] > s.len[2]) return false;
+    if (s.chunk && (s.npass != 3 || s.chunk < s.cols[0] || s.chunk > s.len[2])) return false;
     return sum == m;
 }
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-static onefft_plan *plan_build(size_t n, int m, int npass, const int *len) {
+static onefft_plan *plan_build(size_t n, int m, const Shape &shape) {
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess) {
@@ -134,16 +157,21 @@ static onefft_plan *plan_build(size_t n, int m, int npass, const int *len) {
     p->n = n;
     p->log2n = m;
     p->device = device;
-    p->npass = npass;
-    for (int i = 0; i < npass; ++i) p->len[i] = len[i];
+    p->npass = shape.npass;
+    p->l2_keep = shape.l2_keep;
+    p->chunk = shape.chunk;
+    for (int i = 0; i < shape.npass; ++i) {
+        p->len[i] = shape.len[i];
+        p->cols[i] = shape.cols[i];
+    }
     // layout: stage tables per pass, then the FP64 tables
     size_t off[3], bytes = 0;
-    for (int i = 0; i < npass; ++i) {
+    for (int i = 0; i < p->npass; ++i) {
         off[i] = bytes;
-        bytes = align256(bytes + sizeof(float2) * (size_t)stage_table_entries_host(len[i]));
+        bytes = align256(bytes + sizeof(float2) * (size_t)stage_table_entries_host(p->len[i]));
     }
     size_t lo_off = bytes, hi_off = bytes;
-    if (npass >= 2) {
+    if (p->npass >= 2) {
         p->lo_bits = m / 2;
         lo_off = bytes;
         bytes = align256(bytes + sizeof(double2) * ((size_t)1 << p->lo_bits));
@@ -163,11 +191,11 @@ static onefft_plan *plan_build(size_t n, int m, int npass, const int *len) {
     cudaStream_t s;
     e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
     if (e == cudaSuccess) {
-        for (int i = 0; i < npass && e == cudaSuccess; ++i) {
+        for (int i = 0; i < p->npass && e == cudaSuccess; ++i) {
             p->stw[i] = (const float2 *)(base + off[i]);
-            e = launch_stage_table((float2 *)(base + off[i]), len[i], s);
+            e = launch_stage_table((float2 *)(base + off[i]), p->len[i], s);
         }
-        if (npass >= 2 && e == cudaSuccess) {
+        if (p->npass >= 2 && e == cudaSuccess) {
             p->tw_lo = (const double2 *)(base + lo_off);
             p->tw_hi = (const double2 *)(base + hi_off);
             e = launch_big_table((double2 *)p->tw_lo, (double2 *)p->tw_hi, m, p->lo_bits, s);
@@ -191,22 +219,37 @@ extern "C" onefft_plan *onefft_plan_create(size_t n) {
         set_error(ONEFFT_ERR_SIZE, "n=%zu is not a power of two in [1, 2^30]", n);
         return nullptr;
     }
-    int npass, len[3];
-    default_split(m, &npass, len);
-    return plan_build(n, m, npass, len);
+    return plan_build(n, m, tuned_shape(m));
 }
 
-extern "C" onefft_plan *onefft_plan_create_split(size_t n, int npass, const int *log2_len) {
+extern "C" onefft_plan *onefft_plan_create_tiles(size_t n, int npass, const int *log2_len, const int *log2_cols,
+                                                 int l2_keep, int log2_chunk) {
     int m;
     if (!size_log2(n, &m)) {
         set_error(ONEFFT_ERR_SIZE, "n=%zu is not a power of two in [1, 2^30]", n);
         return nullptr;
     }
-    if (!log2_len || !valid_split(m, npass, log2_len)) {
+    if (!log2_len || npass < 1 || npass > 3) {
         set_error(ONEFFT_ERR_ARG, "invalid pass split for n=%zu", n);
         return nullptr;
     }
-    return plan_build(n, m, npass, log2_len);
+    Shape s{};
+    s.npass = npass;
+    s.l2_keep = l2_keep ? 1 : 0;
+    s.chunk = log2_chunk > 0 ? log2_chunk : 0;
+    for (int i = 0; i < npass; ++i) {
+        s.len[i] = log2_len[i];
+        s.cols[i] = log2_cols ? log2_cols[i] : pass_log_c(log2_len[i]);
+    }
+    if (!valid_shape(m, s)) {
+        set_error(ONEFFT_ERR_ARG, "invalid pass split for n=%zu", n);
+        return nullptr;
+    }
+    return plan_build(n, m, s);
+}
+
+extern "C" onefft_plan *onefft_plan_create_split(size_t n, int npass, const int *log2_len) {
+    return onefft_plan_create_tiles(n, npass, log2_len, nullptr, 1, 0);
 }
 
 extern "C" void onefft_plan_destroy(onefft_plan *plan) {
@@ -250,6 +293,53 @@ static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *
     a.tw_lo = p->tw_lo;
     a.tw_hi = p->tw_hi;
     a.lo_bits = p->lo_bits;
+    a.l2_keep = p->l2_keep;
+    a.tli = 31;
+    if (p->npass == 3 && p->chunk > 0) {
+        // Passes 0 and 1 of a three-pass transform n = A B C run chunk by chunk over the last
+        // digit j_c: pass 1 on columns j_c needs only pass 0's outputs for the same j_c, which
+        // form one contiguous region of A B 2^chunk values, small enough to stay in L2 between
+        // the two launches. Pass 2 then runs over the whole array.
+        const int A = p->len[0], B = p->len[1], Cd = p->len[2], G = p->chunk;
+        PassArgs c0 = a, c1 = a;
+        c0.in = in;
+        c0.out = out;
+        c0.stw = p->stw[0];
+        c0.swap_in = inverse;
+        c0.swap_out = 0;
+        c0.log_s = p->log2n - A;
+        c0.rev_b1 = B;
+        c0.rev_b2 = Cd;
+        c0.tli = G - p->cols[0];
+        c0.outer_shift = Cd;
+        c0.outer_base = 0;
+        c0.ntiles = 1u << (B + G - p->cols[0]);
+        c1.in = out;
+        c1.out = out;
+        c1.stw = p->stw[1];
+        c1.swap_in = c1.swap_out = 0;
+        c1.log_s = A;
+        c1.tli = A - p->cols[1];
+        c1.outer_shift = A;
+        c1.inner_base = 0;
+        c1.ntiles = 1u << (G + A - p->cols[1]);
+        for (unsigned g = 0; g < (1u << Cd); g += 1u << G) {
+            c0.inner_base = g;
+            c1.outer_base = g;
+            g_launches.fetch_add(2);
+            cudaError_t e = launch_pass(0, A, p->cols[0], c0, (int)batch, s);
+            if (e == cudaSuccess) e = launch_pass(1, B, p->cols[1], c1, (int)batch, s);
+            if (e != cudaSuccess) return e;
+        }
+        a.in = out;
+        a.out = out;
+        a.stw = p->stw[2];
+        a.swap_in = 0;
+        a.swap_out = inverse;
+        a.log_s = A + B;
+        g_launches.fetch_add(1);
+        return launch_pass(2, Cd, p->cols[2], a, (int)batch, s);
+    }
     int done = 0;  // log2 of the digits transformed so far
     for (int i = 0; i < p->npass; ++i) {
         const bool first = i == 0, last = i == p->npass - 1;
@@ -267,7 +357,7 @@ static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *
         }
         int mode = first ? 0 : last ? 2 : 1;
         g_launches.fetch_add(1);
-        cudaError_t e = launch_pass(mode, p->len[i], a, (int)batch, s);
+        cudaError_t e = launch_pass(mode, p->len[i], p->cols[i], a, (int)batch, s);
         if (e != cudaSuccess) return e;
         done += p->len[i];
     }

@@ -200,12 +200,20 @@ SPLITS = [
 ]
 
 
-@pytest.mark.parametrize("n,split", SPLITS)
-def test_pass_splits(ofb, oracle, n, split):
-    """Every pass kernel (all tile lengths 2^4..2^12, first/middle/last) against FP64."""
+SHAPES = [  # (n, split, tile widths, chunk)
+    (1 << 12, (4, 4, 4), (2, 3, 2), 2), (1 << 15, (4, 5, 6), (4, 4, 4), 4), (1 << 18, (6, 6, 6), (3, 3, 3), 3),
+    (1 << 16, (8, 8), (2, 2), 0), (1 << 16, (8, 8), (3, 4), 0), (1 << 20, (10, 10), (4, 3), 0),
+    (1 << 21, (7, 7, 7), (4, 4, 4), 5), (1 << 24, (8, 8, 8), (4, 4, 4), 6), (1 << 22, (12, 5, 5), (2, 4, 4), 3),
+]
+
+
+@pytest.mark.parametrize("n,split,cols,chunk", [(n, s, None, 0) for n, s in SPLITS] + SHAPES)
+def test_pass_splits(ofb, oracle, n, split, cols, chunk):
+    """Every pass kernel (all tile lengths 2^4..2^12, widths 4..16, first/middle/last, chunked
+    first passes) against FP64."""
     log2n = n.bit_length() - 1
     x = oracle.gen_normal(2 * n, 1000 + log2n)
-    plan = ofb.Plan(n, split=split)
+    plan = ofb.Plan(n, split=split, cols=cols, chunk=chunk)
     assert plan.passes() == split
     default = ofb.Plan(n)
     for inv in (False, True):
