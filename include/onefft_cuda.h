@@ -72,6 +72,35 @@ ONEFFT_API onefft_plan *onefft_plan_create_tiles(size_t n, int npass, const int 
 /* Number of passes of a plan and their log2 lengths (up to 3 are written to log2_len). */
 ONEFFT_API int onefft_plan_passes(const onefft_plan *plan, int *log2_len);
 
+/* ---- uneven batches ----------------------------------------------------------------------------
+ * Counterpart of a caller looping over OneFFT's onefft_plan_forward/_inverse with a different
+ * plan per size (src/onefft.c:1138-1140): many transforms of different power-of-two sizes packed
+ * in one buffer, run by ONE persistent kernel launch that pulls work from a device queue. The
+ * counter reset and the launch form a CUDA graph built by onefft_uneven_create() and replayed by
+ * each execute. Transform i has size 2^log2n (0 <= log2n <= 16), starts at complex offset
+ * `offset` of both buffers, and runs forward (inverse = 0) or inverse (inverse = 1). Transforms
+ * must not overlap each other. */
+typedef struct onefft_desc {
+    int32_t log2n;
+    int32_t inverse;
+    int64_t offset;
+} onefft_desc;
+
+typedef struct onefft_uneven onefft_uneven;
+
+/* Validates the descriptors (host memory), copies them to the device sorted largest first,
+ * builds the tables of every size used on the current device and the launch graph. Returns
+ * NULL on invalid descriptors (reason in onefft_last_error()) or on allocation failure. */
+ONEFFT_API onefft_uneven *onefft_uneven_create(const onefft_desc *desc, size_t count);
+/* NULL is allowed. */
+ONEFFT_API void onefft_uneven_destroy(onefft_uneven *batch);
+/* Complex values the descriptors span: max over i of offset + 2^log2n. */
+ONEFFT_API size_t onefft_uneven_span(const onefft_uneven *batch);
+/* Runs the whole batch from d_in to d_out (device buffers of at least onefft_uneven_span()
+ * complex values, 8-byte aligned, not overlapping) on `stream`. The batch object holds the work
+ * queue counter, so one batch object must not execute on two streams at once. */
+ONEFFT_API int onefft_uneven_execute(onefft_uneven *batch, const float *d_in, float *d_out, void *stream);
+
 /* ---- information and testing hooks -------------------------------------------------------------*/
 
 /* Message of the last error in the calling thread ("" if none). */

@@ -32,6 +32,7 @@ C_SYMBOLS = (
     "onefft_dev_forward_batched", "onefft_dev_inverse_batched", "onefft_dev_adjoint_batched",
     "onefft_plan_forward_batched", "onefft_plan_inverse_batched",
     "onefft_plan_create_split", "onefft_plan_create_tiles", "onefft_plan_passes",
+    "onefft_uneven_create", "onefft_uneven_destroy", "onefft_uneven_span", "onefft_uneven_execute",
     "onefft_last_error", "onefft_debug_fail_alloc", "onefft_debug_twiddles", "onefft_debug_launch_count",
 )
 
@@ -82,6 +83,14 @@ def lib() -> ctypes.CDLL:
         f = getattr(L, name)
         f.argtypes = [_vp, _vp, _vp, _sz]
         f.restype = ctypes.c_int
+    L.onefft_uneven_create.argtypes = [_vp, _sz]
+    L.onefft_uneven_create.restype = _vp
+    L.onefft_uneven_destroy.argtypes = [_vp]
+    L.onefft_uneven_destroy.restype = None
+    L.onefft_uneven_span.argtypes = [_vp]
+    L.onefft_uneven_span.restype = _sz
+    L.onefft_uneven_execute.argtypes = [_vp, _vp, _vp, _vp]
+    L.onefft_uneven_execute.restype = ctypes.c_int
     L.onefft_last_error.argtypes = []
     L.onefft_last_error.restype = ctypes.c_char_p
     L.onefft_debug_fail_alloc.argtypes = [ctypes.c_int]
@@ -244,5 +253,46 @@ class Plan:
             raise RuntimeError(f"onefft_dev_adjoint_batched failed ({rc}): {last_error()}")
 
 
-__all__ = ["forward", "inverse", "cache_prepare", "cache_clear", "Plan", "implementation", "last_error",
-           "lib", "LIB_PATH", "C_SYMBOLS"]
+DESC_DTYPE = np.dtype([("log2n", np.int32), ("inverse", np.int32), ("offset", np.int64)])
+
+
+class UnevenBatch:
+    """Many transforms of different power-of-two sizes run by one persistent launch
+    (onefft_uneven_* in include/onefft_cuda.h). `desc` is a structured array of DESC_DTYPE, or
+    three sequences (log2n, inverse, offset)."""
+
+    def __init__(self, log2n, inverse=None, offset=None):
+        if inverse is None:
+            d = np.ascontiguousarray(log2n, DESC_DTYPE)
+        else:
+            d = np.empty(len(log2n), DESC_DTYPE)
+            d["log2n"], d["inverse"], d["offset"] = log2n, inverse, offset
+        self.desc = d
+        h = lib().onefft_uneven_create(d.ctypes.data, d.size)
+        if not h:
+            raise ValueError(f"invalid uneven batch: {last_error()}")
+        self._h = h
+
+    @property
+    def span(self) -> int:
+        return int(lib().onefft_uneven_span(self._h))
+
+    def execute(self, d_in: int, d_out: int, stream: int = 0) -> None:
+        rc = lib().onefft_uneven_execute(self._h, d_in, d_out, stream)
+        if rc != 0:
+            raise RuntimeError(f"onefft_uneven_execute failed ({rc}): {last_error()}")
+
+    def destroy(self) -> None:
+        if getattr(self, "_h", None):
+            lib().onefft_uneven_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+__all__ = ["forward", "inverse", "cache_prepare", "cache_clear", "Plan", "UnevenBatch", "DESC_DTYPE",
+           "implementation", "last_error", "lib", "LIB_PATH", "C_SYMBOLS"]

@@ -1,0 +1,180 @@
+// Tile bodies shared by the stand-alone kernels (fft_kernels.cu) and the persistent uneven-batch
+// kernel (uneven.cu): the same arithmetic in both, so an uneven batch reproduces the plain
+// per-size path.
+#pragma once
+
+#include "fft_device.cuh"
+#include "fft_launch.h"
+
+namespace ofb {
+
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+
+// w_n^t for t < n from the two-level tables, in FP64.
+__device__ __forceinline__ double2 big_twiddle_f64(const double2* __restrict__ lo, const double2* __restrict__ hi,
+                                                   int lo_bits, unsigned t) {
+    return zmul(__ldg(lo + (t & ((1u << lo_bits) - 1))), __ldg(hi + (t >> lo_bits)));
+}
+
+// L2 cache hints: the input of a transform is read exactly once (evict first); the intermediate
+// array between passes may be kept in L2 for the next pass (evict last).
+__device__ __forceinline__ float2 ld_stream(const float2* p) { return __ldcs(p); }
+__device__ __forceinline__ unsigned long long policy_evict_last() {
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ void st_policy(float2* p, float2 v, unsigned long long pol) {
+    asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(p), "f"(v.x), "f"(v.y), "l"(pol)
+                 : "memory");
+}
+
+// Shared memory (bytes) of a tile of 2^log_c columns of length 2^log_l, with padding.
+__host__ __device__ constexpr int smem_bytes(int log_l, int log_c) {
+    return (int)sizeof(float2) * ((1 << (log_l + log_c)) + (1 << (log_l + log_c - 4)));
+}
+// ... plus the inter-pass twiddle factors of a pass tile (17 per column).
+__host__ __device__ constexpr int pass_smem_bytes(int log_l, int log_c, int mode) {
+    return smem_bytes(log_l, log_c) + (mode == 2 ? 0 : (int)sizeof(float2) * 17 * (1 << log_c));
+}
+
+// ---- n <= 8: one transform per thread -------------------------------------------------------------
+
+template <int LOG_N>
+__device__ __forceinline__ void tiny_transform(const float2* __restrict__ src, float2* __restrict__ dst, int inverse) {
+    constexpr int N = 1 << LOG_N;
+    float2 a[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        a[i] = __ldg(src + i);
+        if (inverse) a[i] = swap_ri(a[i]);
+    }
+    dft<N>(a);
+#pragma unroll
+    for (int i = 0; i < N; ++i) dst[i] = inverse ? swap_ri(a[i]) : a[i];
+}
+
+// ---- one block of whole transforms, n = 16 .. 2^14 --------------------------------------------------
+//
+// 2^LOG_C transforms of length L = 2^LOG_L, 16 values per thread, thread tid owns column
+// c = tid / (L/16) and butterfly lane j = tid mod (L/16). src / dst point at this thread's
+// transform; inactive columns (past the end of a batch) compute on zeros and store nothing.
+template <int LOG_L, int LOG_C>
+__device__ __forceinline__ void batched_tile(const float2* __restrict__ src, float2* __restrict__ dst, bool active,
+                                             int inverse, const float2* __restrict__ stw, float2* smem, int tid) {
+    constexpr int L = 1 << LOG_L, T = L / 16;
+    const int j = tid & (T - 1);
+    const int c = tid >> (LOG_L - 4);
+    src += j;
+    dst += j;
+    float2 v[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        float2 x = active ? ld_stream(src + T * k) : make_float2(0.f, 0.f);
+        v[k] = inverse ? swap_ri(x) : x;
+    }
+    tile_fft<LOG_L, 1>(v, j, stw, smem, c << LOG_L);
+    if (active) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) dst[T * k] = inverse ? swap_ri(v[k]) : v[k];
+    }
+}
+
+// ---- one tile of a pass of the multi-pass decomposition -----------------------------------------
+//
+// MODE 0: first pass, in -> out with digit-reversed contiguous column runs and w_n^(r k).
+// MODE 1: middle pass, in place on out, twiddle w_n^((h k) S).
+// MODE 2: last pass, in place on out, no twiddle.
+// Tile t covers 2^LOG_C adjacent columns of the transform at element offset `toff`; tid runs
+// over the 2^LOG_C L / 16 threads of the tile.
+template <int LOG_L, int LOG_C, int MODE>
+__device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long long toff, float2* smem, int tid) {
+    constexpr int L = 1 << LOG_L, T = L / 16, C = 1 << LOG_C;
+    const int c = tid & (C - 1);
+    const int j = tid >> LOG_C;
+    const unsigned col0 = a.tli >= 31 ? (t << LOG_C)
+                                      : ((a.outer_base + (t >> a.tli)) << a.outer_shift) + a.inner_base +
+                                            ((t & ((1u << a.tli) - 1)) << LOG_C);
+    unsigned base;  // element e of this thread's column is at base + (e << a.log_s)
+    if (MODE == 0) {
+        base = col0 + c;
+    } else {
+        unsigned q = (col0 & ((1u << a.log_s) - 1)) + c;
+        unsigned h = col0 >> a.log_s;
+        base = q + (h << (a.log_s + LOG_L));
+    }
+    // Inter-pass twiddles w_n^(F (j + T kk)) for this thread's outputs, F = r (first pass,
+    // per column) or S h (middle pass, per tile), split as w^(F j) * w^(F T kk): the 16 factors
+    // w^(F T kk) of each column are evaluated once per tile from the FP64 tables into shared
+    // memory (rows padded to 17 so the columns of a warp hit distinct banks), w^(F j) once per
+    // thread; each is rounded once to FP32 and their product applied in FP32.
+    float2* tws = smem + spad(C * L - 1) + 1;
+    if (MODE != 2) {
+        const unsigned hs = (col0 >> a.log_s) << a.log_s;
+        for (int i = tid; i < (MODE == 0 ? C : 1) * 16; i += C * T) {
+            const int cc = i >> 4, kk = i & 15;
+            const unsigned f = MODE == 0 ? col0 + cc : hs;
+            double2 w = big_twiddle_f64(a.tw_lo, a.tw_hi, a.lo_bits, f * (unsigned)T * (unsigned)kk);
+            tws[cc * 17 + kk] = make_float2((float)w.x, (float)w.y);
+        }
+    }
+    // element j + T k of the column: p0 + k * estep
+    const long long estep = (long long)T << a.log_s;
+    const long long off0 = toff + base + ((long long)j << a.log_s);
+    float2 v[16];
+    {
+        const float2* p0 = a.in + off0;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            // The first pass streams the input, which is never read again. Later passes read
+            // and write `out` in place, so they avoid the read-only cache path.
+            float2 x = MODE == 0 ? ld_stream(p0 + k * estep) : p0[k * estep];
+            v[k] = a.swap_in ? swap_ri(x) : x;
+        }
+    }
+    tile_fft<LOG_L, C>(v, j, a.stw, smem, c);
+    if (MODE != 2) {
+        if (Stages<LOG_L>::COUNT == 1) __syncthreads();  // tile_fft had no barrier to publish tws
+        const unsigned f = MODE == 0 ? col0 + c : (col0 >> a.log_s) << a.log_s;
+        const double2 wj = big_twiddle_f64(a.tw_lo, a.tw_hi, a.lo_bits, f * (unsigned)j);
+        const float2 wjf = make_float2((float)wj.x, (float)wj.y);
+        const float2* tw = tws + (MODE == 0 ? c * 17 : 0);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[k] = cmul(v[k], cmul(wjf, tw[k]));
+    }
+    const unsigned long long keep = a.l2_keep ? policy_evict_last() : 0ull;
+    if (MODE == 0) {
+        // Transpose through shared memory so that each column's L results leave as one
+        // contiguous, coalesced run: thread tid then stores values kk0 + T i (i = 0..15) of
+        // column cc = tid / T, at its digit-reversed place.
+        {
+            float2* w = smem + spad(j * C + c);
+#pragma unroll
+            for (int k = 0; k < 16; ++k) w[padc(k * T * C)] = v[k];
+        }
+        __syncthreads();
+        const int cc = tid >> (LOG_L - 4), kk0 = tid & (T - 1);
+        const unsigned rr = col0 + cc;
+        const unsigned j2 = rr & ((1u << a.rev_b2) - 1), j1 = rr >> a.rev_b2;
+        float2* q = a.out + toff + (((j1 + (j2 << a.rev_b1)) << LOG_L) + kk0);
+        const float2* r = smem + spad(kk0 * C + cc);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            float2 x = r[padc(i * T * C)];
+            if (a.l2_keep) st_policy(q + i * T, x, keep);
+            else q[i * T] = x;
+        }
+    } else {
+        float2* p0 = a.out + off0;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            float2 x = a.swap_out ? swap_ri(v[k]) : v[k];
+            if (MODE == 1 && a.l2_keep) st_policy(p0 + k * estep, x, keep);
+            else p0[k * estep] = x;
+        }
+    }
+}
+
+}  // namespace ofb

@@ -22,8 +22,13 @@
 #include <new>
 #include <string>
 
-#include "../../include/onefft_cuda.h"
+#include "onefft_cuda.h"
 #include "fft_launch.h"
+#include "uneven.h"
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
 
 using namespace ofb;
 
@@ -103,6 +108,24 @@ struct Shape {
     int chunk;
 };
 
+// Fastest shapes measured on a B200 by onefft_b200/autotune.py (forward transform, L2 flushed
+// before each repetition): {npass, {log2 lengths}, {log2 tile widths}, l2_keep, chunk}.
+static const Shape kTuned[] = {
+    /* 15 */ {2, {8, 7, 0}, {3, 4, 0}, 1, 0},
+    /* 16 */ {2, {8, 8, 0}, {3, 3, 0}, 1, 0},
+    /* 17 */ {2, {9, 8, 0}, {2, 3, 0}, 1, 0},
+    /* 18 */ {2, {8, 10, 0}, {4, 2, 0}, 1, 0},
+    /* 19 */ {2, {8, 11, 0}, {4, 2, 0}, 0, 0},
+    /* 20 */ {2, {10, 10, 0}, {2, 3, 0}, 0, 0},
+    /* 21 */ {2, {11, 10, 0}, {3, 4, 0}, 1, 0},
+    /* 22 */ {3, {7, 7, 8}, {4, 4, 4}, 1, 0},
+    /* 23 */ {3, {8, 8, 7}, {3, 3, 4}, 0, 0},
+    /* 24 */ {3, {8, 8, 8}, {4, 4, 4}, 0, 0},
+    /* 25 */ {3, {8, 9, 8}, {4, 3, 4}, 0, 0},
+    /* 26 */ {3, {8, 9, 9}, {4, 3, 4}, 1, 0},
+    /* 27 */ {3, {9, 9, 9}, {4, 3, 4}, 1, 0},
+};
+
 static Shape tuned_shape(int m) {
     Shape s{};
     if (m <= kMaxSingleLog2) {
@@ -110,6 +133,7 @@ static Shape tuned_shape(int m) {
         s.len[0] = m;
         return s;
     }
+    if (m >= 15 && m <= 27) return kTuned[m - 15];
     if (m <= 24) {
         s.npass = 2;
         s.len[0] = (m + 1) / 2;
@@ -657,4 +681,195 @@ extern "C" int onefft_debug_twiddles(unsigned log2n, size_t count, float *out) {
     if (e == cudaSuccess) e = cudaMemcpy(out, d, count * sizeof(float2), cudaMemcpyDeviceToHost);
     cudaFree(d);
     return e == cudaSuccess ? 0 : cuda_error(e, "twiddle probe");
+}
+
+// ---- uneven batches (kernel in uneven.cu) --------------------------------------------------------
+
+struct onefft_uneven {
+    int device;
+    size_t count;
+    size_t span;
+    onefft_plan *plans[kUnevenMaxLog2 + 1];
+    void *mem;  // sorted descriptors, work items, queue counter
+    UnevenArgs args;
+    int grid;
+    int smem;
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    cudaGraphNode_t knode;
+};
+
+extern "C" void onefft_uneven_destroy(onefft_uneven *u) {
+    if (!u) return;
+    if (u->exec) cudaGraphExecDestroy(u->exec);
+    if (u->graph) cudaGraphDestroy(u->graph);
+    if (u->mem) cudaFree(u->mem);
+    for (int m = 0; m <= kUnevenMaxLog2; ++m) onefft_plan_destroy(u->plans[m]);
+    delete u;
+}
+
+extern "C" size_t onefft_uneven_span(const onefft_uneven *u) { return u ? u->span : 0; }
+
+extern "C" onefft_uneven *onefft_uneven_create(const onefft_desc *desc, size_t count) {
+    t_last_error.clear();
+    if (!desc || count == 0 || count > (size_t)1 << 30) {
+        set_error(ONEFFT_ERR_ARG, "invalid descriptor list");
+        return nullptr;
+    }
+    // validate, then check that no two transforms overlap
+    std::vector<size_t> by_offset(count);
+    size_t span = 0;
+    for (size_t i = 0; i < count; ++i) {
+        const onefft_desc &d = desc[i];
+        if (d.log2n < 0 || d.log2n > kUnevenMaxLog2 || (d.inverse != 0 && d.inverse != 1) || d.offset < 0 ||
+            d.offset > ((int64_t)1 << 40)) {
+            set_error(ONEFFT_ERR_ARG, "descriptor %zu invalid (log2n %d, inverse %d, offset %lld)", i, d.log2n,
+                      d.inverse, (long long)d.offset);
+            return nullptr;
+        }
+        span = std::max(span, (size_t)d.offset + ((size_t)1 << d.log2n));
+        by_offset[i] = i;
+    }
+    std::sort(by_offset.begin(), by_offset.end(),
+              [desc](size_t a, size_t b) { return desc[a].offset < desc[b].offset; });
+    for (size_t i = 1; i < count; ++i) {
+        const onefft_desc &p = desc[by_offset[i - 1]], &q = desc[by_offset[i]];
+        if (p.offset + ((int64_t)1 << p.log2n) > q.offset) {
+            set_error(ONEFFT_ERR_ARG, "transforms at offsets %lld and %lld overlap", (long long)p.offset,
+                      (long long)q.offset);
+            return nullptr;
+        }
+    }
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) {
+        cuda_error(e, "no CUDA device");
+        return nullptr;
+    }
+    onefft_uneven *u = new (std::nothrow) onefft_uneven();
+    if (!u) {
+        set_error(ONEFFT_ERR_SIZE, "out of host memory");
+        return nullptr;
+    }
+    u->device = device;
+    u->count = count;
+    u->span = span;
+    // largest transforms first, then by offset; equal sizes grouped into work items
+    std::vector<onefft_desc> sorted(desc, desc + count);
+    std::stable_sort(sorted.begin(), sorted.end(), [](const onefft_desc &a, const onefft_desc &b) {
+        return a.log2n != b.log2n ? a.log2n > b.log2n : a.offset < b.offset;
+    });
+    std::vector<UnevenItem> items;
+    for (size_t i = 0; i < count;) {
+        const int m = sorted[i].log2n;
+        const size_t cap = m <= 3 ? 256 : m <= 12 ? ((size_t)4096 >> m) : 1;
+        size_t k = 0;
+        while (i + k < count && sorted[i + k].log2n == m && k < cap) ++k;
+        items.push_back(UnevenItem{m, (int)k, (int)i, 0});
+        i += k;
+    }
+    // tables of every size used: the plain single-kernel plan up to 2^12, the in-block two-pass
+    // split beyond
+    bool used[kUnevenMaxLog2 + 1] = {};
+    for (const onefft_desc &d : sorted) used[d.log2n] = true;
+    for (int m = 0; m <= kUnevenMaxLog2; ++m) {
+        if (!used[m]) continue;
+        if (m <= 12) {
+            u->plans[m] = onefft_plan_create((size_t)1 << m);
+        } else {
+            const int len[2] = {uneven_split(m, 0), uneven_split(m, 1)};
+            u->plans[m] = onefft_plan_create_tiles((size_t)1 << m, 2, len, nullptr, 0, 0);
+        }
+        if (!u->plans[m]) {
+            onefft_uneven_destroy(u);
+            set_error(ONEFFT_ERR_SIZE, "table build for 2^%d failed", m);
+            return nullptr;
+        }
+        const onefft_plan *p = u->plans[m];
+        u->args.stw[m][0] = p->stw[0];
+        u->args.stw[m][1] = p->npass > 1 ? p->stw[1] : nullptr;
+        u->args.tw_lo[m] = p->tw_lo;
+        u->args.tw_hi[m] = p->tw_hi;
+        u->args.lo_bits[m] = p->lo_bits;
+    }
+    const size_t desc_bytes = align256(count * sizeof(onefft_desc));
+    const size_t item_bytes = align256(items.size() * sizeof(UnevenItem));
+    e = dev_alloc(&u->mem, desc_bytes + item_bytes + 256);
+    if (e != cudaSuccess) {
+        u->mem = nullptr;
+        onefft_uneven_destroy(u);
+        set_error(ONEFFT_ERR_SIZE, "uneven batch allocation failed");
+        return nullptr;
+    }
+    char *base = (char *)u->mem;
+    u->args.desc = (const onefft_desc *)base;
+    u->args.items = (const UnevenItem *)(base + desc_bytes);
+    u->args.counter = (int *)(base + desc_bytes + item_bytes);
+    u->args.nitems = (int)items.size();
+    e = cudaMemcpy(base, sorted.data(), count * sizeof(onefft_desc), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(base + desc_bytes, items.data(), items.size() * sizeof(UnevenItem), cudaMemcpyHostToDevice);
+    // persistent grid: every block resident at once
+    u->smem = uneven_smem_bytes();
+    int per_sm = 0, sms = 0;
+    if (e == cudaSuccess && u->smem > 48 * 1024)
+        e = cudaFuncSetAttribute(uneven_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, u->smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, uneven_kernel(), 256, u->smem);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    u->grid = std::max(1, std::min(per_sm * sms, (int)items.size()));
+    // graph: zero the queue counter, then the persistent launch
+    if (e == cudaSuccess) e = cudaGraphCreate(&u->graph, 0);
+    cudaGraphNode_t mset = nullptr;
+    if (e == cudaSuccess) {
+        cudaMemsetParams mp{};
+        mp.dst = u->args.counter;
+        mp.value = 0;
+        mp.elementSize = 4;
+        mp.width = 1;
+        mp.height = 1;
+        e = cudaGraphAddMemsetNode(&mset, u->graph, nullptr, 0, &mp);
+    }
+    if (e == cudaSuccess) {
+        void *params[1] = {&u->args};
+        cudaKernelNodeParams kp{};
+        kp.func = (void *)uneven_kernel();
+        kp.gridDim = dim3((unsigned)u->grid);
+        kp.blockDim = dim3(256);
+        kp.sharedMemBytes = (unsigned)u->smem;
+        kp.kernelParams = params;
+        e = cudaGraphAddKernelNode(&u->knode, u->graph, &mset, 1, &kp);
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&u->exec, u->graph, 0);
+    if (e != cudaSuccess) {
+        onefft_uneven_destroy(u);
+        cuda_error(e, "uneven batch setup");
+        return nullptr;
+    }
+    return u;
+}
+
+extern "C" int onefft_uneven_execute(onefft_uneven *u, const float *d_in, float *d_out, void *stream) {
+    t_last_error.clear();
+    if (!u) return set_error(ONEFFT_ERR_ARG, "NULL batch");
+    if (!d_in || !d_out) return set_error(ONEFFT_ERR_ARG, "NULL buffer");
+    if (((uintptr_t)d_in | (uintptr_t)d_out) & 7) return set_error(ONEFFT_ERR_ARG, "device buffers must be 8-byte aligned");
+    if (ranges_overlap(d_in, d_out, u->span * sizeof(float2))) return set_error(ONEFFT_ERR_ARG, "input and output overlap");
+    cudaError_t e = cudaSuccess;
+    if (u->args.in != (const float2 *)d_in || u->args.out != (float2 *)d_out) {
+        u->args.in = (const float2 *)d_in;
+        u->args.out = (float2 *)d_out;
+        void *params[1] = {&u->args};
+        cudaKernelNodeParams kp{};
+        kp.func = (void *)uneven_kernel();
+        kp.gridDim = dim3((unsigned)u->grid);
+        kp.blockDim = dim3(256);
+        kp.sharedMemBytes = (unsigned)u->smem;
+        kp.kernelParams = params;
+        e = cudaGraphExecKernelNodeSetParams(u->exec, u->knode, &kp);
+    }
+    if (e == cudaSuccess) {
+        g_launches.fetch_add(1);
+        e = cudaGraphLaunch(u->exec, (cudaStream_t)stream);
+    }
+    return e == cudaSuccess ? 0 : cuda_error(e, "uneven batch launch");
 }

@@ -92,6 +92,26 @@ def test_device_calls_reject_bad_arguments_without_device(cuda_lib):
     assert cuda_lib.onefft_plan_forward_batched(None, 0, 0, 1) == -2
 
 
+def test_uneven_descriptors_validated_on_host(cuda_lib):
+    """Invalid uneven-batch descriptors are rejected before any device work."""
+    import onefft_b200 as ofb
+    bad = [
+        ([17], [0], [0]),          # size beyond 2^16
+        ([4], [2], [0]),           # direction not 0/1
+        ([4], [0], [-1]),          # negative offset
+        ([4, 4], [0, 1], [0, 15]),  # overlapping transforms
+    ]
+    for log2n, inv, off in bad:
+        d = np.empty(len(log2n), ofb.DESC_DTYPE)
+        d["log2n"], d["inverse"], d["offset"] = log2n, inv, off
+        assert cuda_lib.onefft_uneven_create(d.ctypes.data, d.size) is None
+        assert cuda_lib.onefft_last_error()
+    assert cuda_lib.onefft_uneven_create(None, 3) is None
+    cuda_lib.onefft_uneven_destroy(None)
+    assert cuda_lib.onefft_uneven_span(None) == 0
+    assert cuda_lib.onefft_uneven_execute(None, 0, 0, None) == -2
+
+
 def test_python_mirror_raises_on_invalid_size(cuda_lib):
     import onefft_b200
     with pytest.raises(ValueError):
