@@ -101,6 +101,21 @@ ONEFFT_API size_t onefft_uneven_span(const onefft_uneven *batch);
  * queue counter, so one batch object must not execute on two streams at once. */
 ONEFFT_API int onefft_uneven_execute(onefft_uneven *batch, const float *d_in, float *d_out, void *stream);
 
+/* The same uneven batch with no device allocation at all, for callers that cannot let a library
+ * call cudaMalloc: real-time threads that must not block in the allocator or hit out-of-memory
+ * after start-up, and applications whose device memory all belongs to their own arena or
+ * budget. It has no counterpart in OneFFT. Instead of a batch object it uses one fixed
+ * 384 KiB __device__ array per GPU (held by every GPU that loads the library until the process
+ * exits) for the twiddle tables of sizes 2^4 .. 2^16, the sorted descriptors and the work
+ * queue. Limits: at most 4096 descriptors per call (more is rejected with -2 and a message in
+ * onefft_last_error()), log2n <= 16, same buffer rules as onefft_uneven_execute(). The first
+ * call on a device builds the tables there (a few small kernels, then a stream synchronize);
+ * make that first call before any stream capture. Later calls only copy the descriptors in,
+ * zero the queue counter and launch. Every call shares the array and overwrites it: calls
+ * whose GPU work overlaps race, so issue them in order (for example on one stream). */
+ONEFFT_API int onefft_uneven_execute_noalloc(const onefft_desc *desc, size_t count, const float *d_in, float *d_out,
+                                             void *stream);
+
 /* ---- information and testing hooks -------------------------------------------------------------*/
 
 /* Message of the last error in the calling thread ("" if none). */

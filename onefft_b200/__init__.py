@@ -33,6 +33,7 @@ C_SYMBOLS = (
     "onefft_plan_forward_batched", "onefft_plan_inverse_batched",
     "onefft_plan_create_split", "onefft_plan_create_tiles", "onefft_plan_passes",
     "onefft_uneven_create", "onefft_uneven_destroy", "onefft_uneven_span", "onefft_uneven_execute",
+    "onefft_uneven_execute_noalloc",
     "onefft_last_error", "onefft_debug_fail_alloc", "onefft_debug_twiddles", "onefft_debug_launch_count",
 )
 
@@ -91,6 +92,8 @@ def lib() -> ctypes.CDLL:
     L.onefft_uneven_span.restype = _sz
     L.onefft_uneven_execute.argtypes = [_vp, _vp, _vp, _vp]
     L.onefft_uneven_execute.restype = ctypes.c_int
+    L.onefft_uneven_execute_noalloc.argtypes = [_vp, _sz, _vp, _vp, _vp]
+    L.onefft_uneven_execute_noalloc.restype = ctypes.c_int
     L.onefft_last_error.argtypes = []
     L.onefft_last_error.restype = ctypes.c_char_p
     L.onefft_debug_fail_alloc.argtypes = [ctypes.c_int]

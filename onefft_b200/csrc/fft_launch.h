@@ -44,6 +44,8 @@ cudaError_t launch_pass(int mode, int log_l, int log_c, const PassArgs& a, int b
 cudaError_t launch_stage_table(float2* dst, int log_l, cudaStream_t stream);
 cudaError_t launch_big_table(double2* lo, double2* hi, int log2n, int lo_bits, cudaStream_t stream);
 int stage_table_entries_host(int log_l);
+// Sets the calling thread's onefft_last_error() message.
+void record_error(const char *msg);
 cudaError_t launch_twiddle_probe(float2* dst, unsigned log2n, unsigned long long count, cudaStream_t stream);
 
 }  // namespace ofb

@@ -49,6 +49,9 @@ static int set_error(int code, const char *fmt, ...) {
     return code;
 }
 
+// Sets the calling thread's onefft_last_error() message (for entry points in other files).
+void ofb::record_error(const char *msg) { t_last_error = msg; }
+
 static int cuda_error(cudaError_t e, const char *what) {
     cudaGetLastError();  // clear a non-sticky error so later calls start clean
     return set_error(ONEFFT_ERR_CUDA_BASE - (int)e, "%s: %s", what, cudaGetErrorString(e));
