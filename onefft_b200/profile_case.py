@@ -1,0 +1,58 @@
+"""Runs one transform shape a few times, for an external profiler (ncu) to capture.
+
+    python -m onefft_b200.profile_case --log2n 24 [--split 8,8,8 --cols 4,4,4] [--batch 1] [--reps 3]
+    python -m onefft_b200.profile_case --log2n 12 --batch 4096            # the batched kernel
+    python -m onefft_b200.profile_case --uneven 2000                      # the uneven-batch kernel
+
+Inputs are seeded standard-normal values on the device; the plan (and its table kernels) is
+built before the timed transforms, so `ncu -k regex:k_pass -s <n>` can skip to them.
+"""
+from __future__ import annotations
+
+import argparse
+
+import numpy as np
+import torch
+
+import onefft_b200 as ofb
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--log2n", type=int, default=12)
+    ap.add_argument("--split", default="")
+    ap.add_argument("--cols", default="")
+    ap.add_argument("--batch", type=int, default=1)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--inverse", action="store_true")
+    ap.add_argument("--uneven", type=int, default=0, help="run an uneven batch of this many transforms")
+    args = ap.parse_args()
+    g = torch.Generator(device="cuda").manual_seed(7)
+    if args.uneven:
+        rng = np.random.default_rng(7)
+        log2n = rng.integers(4, 17, args.uneven).astype(np.int32)
+        inv = (rng.random(args.uneven) < 0.5).astype(np.int32)
+        off = np.concatenate([[0], np.cumsum(1 << log2n.astype(np.int64))[:-1]])
+        b = ofb.UnevenBatch(log2n, inv, off)
+        x = torch.randn(2 * b.span, device="cuda", generator=g)
+        y = torch.empty_like(x)
+        for _ in range(args.reps):
+            b.execute(x.data_ptr(), y.data_ptr())
+        torch.cuda.synchronize()
+        print(f"uneven batch of {args.uneven} transforms, {b.span} values: {args.reps} runs")
+        return
+    n = 1 << args.log2n
+    split = tuple(int(v) for v in args.split.split(",")) if args.split else None
+    cols = tuple(int(v) for v in args.cols.split(",")) if args.cols else None
+    plan = ofb.Plan(n, split=split, cols=cols)
+    x = torch.randn(2 * n * args.batch, device="cuda", generator=g)
+    y = torch.empty_like(x)
+    f = plan.dev_inverse if args.inverse else plan.dev_forward
+    for _ in range(args.reps):
+        f(x.data_ptr(), y.data_ptr(), args.batch)
+    torch.cuda.synchronize()
+    print(f"n=2^{args.log2n} x {args.batch}, passes {plan.passes()}: {args.reps} runs")
+
+
+if __name__ == "__main__":
+    main()
