@@ -217,6 +217,7 @@ def main():
     import torch
 
     import onefft_b200 as ofb
+    from onefft_b200.shard import max_over_ranks
 
     torch.cuda.set_device(local_rank)
     dist = None
@@ -280,10 +281,7 @@ def main():
     launches = int(L.onefft_debug_launch_count() - launches0)
     clk = clocks.stop()
     t = events[0][0].elapsed_time(events[-1][-1]) / 1e3
-    if dist:
-        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t = tt.item()
+    t = max_over_ranks(t, device="cuda")
     per_step = t / args.steps
     value = world * STEP_FLOPS / per_step / 1e9
     peak, peak_kind = measured_peaks()
@@ -345,10 +343,7 @@ def main():
         for _ in range(e2e_steps):
             e2e_step()
         t_e2e = (time.perf_counter() - t0) / e2e_steps
-        if dist:
-            tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t_e2e = tt.item()
+        t_e2e = max_over_ranks(t_e2e, device="cuda")
         same = all(torch.equal(hy[:4096].cuda(), w["y"][:4096]) for w, hx, hy, hz in host)
         nbytes = sum(2 * 8 * (1 << w["log2n"]) * w["batch"] for w in work)
         e2e = {"value": world * STEP_FLOPS / t_e2e / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": nbytes,
