@@ -69,6 +69,17 @@ ONEFFT_API onefft_plan *onefft_plan_create_split(size_t n, int npass, const int 
 ONEFFT_API onefft_plan *onefft_plan_create_tiles(size_t n, int npass, const int *log2_len, const int *log2_cols,
                                                  int l2_keep, int log2_chunk);
 
+/* ---- split-BF16 tensor-core variant --------------------------------------------------------------
+ * A plan whose radix-16 stages run as dense complex 16x16 matrix products on the tensor cores:
+ * BF16 operands split into hi + lo parts, three-term products (hi hi + hi lo + lo hi) accumulated
+ * in FP32; twiddles and the last radix-2/4/8 stage stay FP32. Same transforms, layouts, entry
+ * points and batching as an FP32 plan. Its error is ~2^-17 per stage (about 100x the FP32
+ * path's), so it is accepted only at sizes where it meets the FP32 path's error bound: with
+ * require_accepted != 0 other sizes return NULL ("does not meet the FP32 error bound"); with 0
+ * the plan is built anyway, for measurement. n must be a power of two in [16, 2^30]. No
+ * counterpart in OneFFT. */
+ONEFFT_API onefft_plan *onefft_plan_create_bf16x3(size_t n, int require_accepted);
+
 /* Number of passes of a plan and their log2 lengths (up to 3 are written to log2_len). */
 ONEFFT_API int onefft_plan_passes(const onefft_plan *plan, int *log2_len);
 

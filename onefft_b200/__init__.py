@@ -31,7 +31,7 @@ C_SYMBOLS = (
     "onefft_plan_size", "onefft_implementation",
     "onefft_dev_forward_batched", "onefft_dev_inverse_batched", "onefft_dev_adjoint_batched",
     "onefft_plan_forward_batched", "onefft_plan_inverse_batched",
-    "onefft_plan_create_split", "onefft_plan_create_tiles", "onefft_plan_passes",
+    "onefft_plan_create_split", "onefft_plan_create_tiles", "onefft_plan_create_bf16x3", "onefft_plan_passes",
     "onefft_uneven_create", "onefft_uneven_destroy", "onefft_uneven_span", "onefft_uneven_execute",
     "onefft_uneven_execute_noalloc",
     "onefft_last_error", "onefft_debug_fail_alloc", "onefft_debug_twiddles", "onefft_debug_launch_count",
@@ -64,6 +64,8 @@ def lib() -> ctypes.CDLL:
     L.onefft_plan_create_tiles.argtypes = [_sz, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                            ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int]
     L.onefft_plan_create_tiles.restype = _vp
+    L.onefft_plan_create_bf16x3.argtypes = [_sz, ctypes.c_int]
+    L.onefft_plan_create_bf16x3.restype = _vp
     L.onefft_plan_destroy.argtypes = [_vp]
     L.onefft_plan_destroy.restype = None
     L.onefft_plan_forward.argtypes = [_vp, _vp, _vp]
@@ -166,11 +168,15 @@ class Plan:
     """Owns the device tables of one size (OneFFT's onefft::Plan, include/onefft.h:136-167)."""
 
     def __init__(self, n: int, split: tuple[int, ...] | None = None, cols: tuple[int, ...] | None = None,
-                 l2_keep: bool = True, chunk: int = 0):
+                 l2_keep: bool = True, chunk: int = 0, bf16x3: bool = False, require_accepted: bool = False):
         """split: log2 pass lengths (None = tuned table); cols: log2 tile widths per pass;
-        chunk: three passes only, log2 last-digit columns per L2-resident chunk (0 = none)."""
+        chunk: three passes only, log2 last-digit columns per L2-resident chunk (0 = none);
+        bf16x3: the split-BF16 tensor-core variant (require_accepted: only at sizes where it
+        meets the FP32 error bound)."""
         L = lib()
-        if split is None:
+        if bf16x3:
+            h = L.onefft_plan_create_bf16x3(n, int(require_accepted))
+        elif split is None:
             h = L.onefft_plan_create(n)
         else:
             arr = (ctypes.c_int * len(split))(*split)

@@ -41,6 +41,11 @@ bool pass_tile_supported(int log_l, int log_c);
 cudaError_t launch_single_kernel(int log2n, const float2* in, float2* out, long long batch, const float2* stw,
                                  int inverse, cudaStream_t stream);
 cudaError_t launch_pass(int mode, int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t stream);
+// split-BF16 tensor-core variants (fft_tc.cu): n = 2^4 .. 2^14 in one kernel; pass lengths
+// 2^5 .. 2^12 with the default tile width pass_log_c()
+cudaError_t launch_single_kernel_tc(int log2n, const float2* in, float2* out, long long batch, const float2* stw,
+                                    int inverse, cudaStream_t stream);
+cudaError_t launch_pass_tc(int mode, int log_l, const PassArgs& a, int batch, cudaStream_t stream);
 cudaError_t launch_stage_table(float2* dst, int log_l, cudaStream_t stream);
 cudaError_t launch_big_table(double2* lo, double2* hi, int log2n, int lo_bits, cudaStream_t stream);
 int stage_table_entries_host(int log_l);

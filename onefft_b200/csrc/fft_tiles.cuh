@@ -5,6 +5,7 @@
 
 #include "fft_device.cuh"
 #include "fft_launch.h"
+#include "fft_tc.cuh"
 
 namespace ofb {
 
@@ -61,7 +62,8 @@ __device__ __forceinline__ void tiny_transform(const float2* __restrict__ src, f
 // 2^LOG_C transforms of length L = 2^LOG_L, 16 values per thread, thread tid owns column
 // c = tid / (L/16) and butterfly lane j = tid mod (L/16). src / dst point at this thread's
 // transform; inactive columns (past the end of a batch) compute on zeros and store nothing.
-template <int LOG_L, int LOG_C>
+// TC selects the split-BF16 tensor-core stages (fft_tc.cuh).
+template <int LOG_L, int LOG_C, bool TC = false>
 __device__ __forceinline__ void batched_tile(const float2* __restrict__ src, float2* __restrict__ dst, bool active,
                                              int inverse, const float2* __restrict__ stw, float2* smem, int tid) {
     constexpr int L = 1 << LOG_L, T = L / 16;
@@ -75,7 +77,8 @@ __device__ __forceinline__ void batched_tile(const float2* __restrict__ src, flo
         float2 x = active ? ld_stream(src + T * k) : make_float2(0.f, 0.f);
         v[k] = inverse ? swap_ri(x) : x;
     }
-    tile_fft<LOG_L, 1>(v, j, stw, smem, c << LOG_L);
+    if constexpr (TC) tile_fft_tc<LOG_L, LOG_C, 1>(v, j, stw, smem, c << LOG_L, tid);
+    else tile_fft<LOG_L, 1>(v, j, stw, smem, c << LOG_L);
     if (active) {
 #pragma unroll
         for (int k = 0; k < 16; ++k) dst[T * k] = inverse ? swap_ri(v[k]) : v[k];
@@ -89,7 +92,7 @@ __device__ __forceinline__ void batched_tile(const float2* __restrict__ src, flo
 // MODE 2: last pass, in place on out, no twiddle.
 // Tile t covers 2^LOG_C adjacent columns of the transform at element offset `toff`; tid runs
 // over the 2^LOG_C L / 16 threads of the tile.
-template <int LOG_L, int LOG_C, int MODE>
+template <int LOG_L, int LOG_C, int MODE, bool TC = false>
 __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long long toff, float2* smem, int tid) {
     constexpr int L = 1 << LOG_L, T = L / 16, C = 1 << LOG_C;
     const int c = tid & (C - 1);
@@ -134,7 +137,8 @@ __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long lo
             v[k] = a.swap_in ? swap_ri(x) : x;
         }
     }
-    tile_fft<LOG_L, C>(v, j, a.stw, smem, c);
+    if constexpr (TC) tile_fft_tc<LOG_L, LOG_C, C>(v, j, a.stw, smem, c, tid);
+    else tile_fft<LOG_L, C>(v, j, a.stw, smem, c);
     if (MODE != 2) {
         if (Stages<LOG_L>::COUNT == 1) __syncthreads();  // tile_fft had no barrier to publish tws
         const unsigned f = MODE == 0 ? col0 + c : (col0 >> a.log_s) << a.log_s;

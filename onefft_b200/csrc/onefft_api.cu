@@ -92,6 +92,7 @@ struct onefft_plan {
     int cols[3];           // log2 of the tile width (columns per block) of each pass
     int l2_keep;           // intermediate stores with L2 evict-last priority
     int chunk;             // three passes: log2 of the last-digit columns per chunk of passes 0+1 (0 = none)
+    int tc;                // radix-16 stages as split-BF16 tensor-core products (onefft_plan_create_bf16x3)
     void *mem;             // the one device allocation
     size_t mem_bytes;
     const float2 *stw[3];  // stage twiddles of each pass's length
@@ -275,6 +276,36 @@ extern "C" onefft_plan *onefft_plan_create_tiles(size_t n, int npass, const int 
     return plan_build(n, m, s);
 }
 
+// Sizes (bit log2 n) at which the split-BF16 tensor-core variant meets the FP32 path's error
+// bound (relative RMS against FP64 at most 2x OneFFT's own). Measured on a B200 with standard
+// normal inputs with 1 % of the values scaled by 1e3 (tests/test_gpu_bf16x3.py): three-term
+// BF16 products leave ~1e-5 relative error, about 100x the bound at every size, so none is.
+static const unsigned long long kBf16x3Accepted = 0;
+
+extern "C" onefft_plan *onefft_plan_create_bf16x3(size_t n, int require_accepted) {
+    int m;
+    if (!size_log2(n, &m) || m < 4) {
+        set_error(ONEFFT_ERR_SIZE, "n=%zu: the tensor-core variant needs a power of two in [16, 2^30]", n);
+        return nullptr;
+    }
+    if (require_accepted && !((kBf16x3Accepted >> m) & 1)) {
+        set_error(ONEFFT_ERR_SIZE, "n=2^%d: split-BF16 does not meet the FP32 error bound at this size", m);
+        return nullptr;
+    }
+    Shape s = tuned_shape(m);
+    s.chunk = 0;
+    for (int i = 0; i < s.npass; ++i) {
+        s.cols[i] = pass_log_c(s.len[i]);
+        if (s.npass > 1 && s.len[i] < 5) {
+            set_error(ONEFFT_ERR_SIZE, "n=2^%d: no tensor-core split", m);
+            return nullptr;
+        }
+    }
+    onefft_plan *p = plan_build(n, m, s);
+    if (p) p->tc = 1;
+    return p;
+}
+
 extern "C" onefft_plan *onefft_plan_create_split(size_t n, int npass, const int *log2_len) {
     return onefft_plan_create_tiles(n, npass, log2_len, nullptr, 1, 0);
 }
@@ -313,6 +344,7 @@ static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *
     if (batch <= 0) return cudaSuccess;
     if (p->npass == 1) {
         g_launches.fetch_add(1);
+        if (p->tc) return launch_single_kernel_tc(p->log2n, in, out, batch, p->stw[0], inverse, s);
         return launch_single_kernel(p->log2n, in, out, batch, p->stw[0], inverse, s);
     }
     PassArgs a{};
@@ -384,7 +416,8 @@ static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *
         }
         int mode = first ? 0 : last ? 2 : 1;
         g_launches.fetch_add(1);
-        cudaError_t e = launch_pass(mode, p->len[i], p->cols[i], a, (int)batch, s);
+        cudaError_t e = p->tc ? launch_pass_tc(mode, p->len[i], a, (int)batch, s)
+                              : launch_pass(mode, p->len[i], p->cols[i], a, (int)batch, s);
         if (e != cudaSuccess) return e;
         done += p->len[i];
     }
