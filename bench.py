@@ -70,6 +70,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-configs", action="store_true")
     return ap.parse_args()
 
 
@@ -203,6 +204,89 @@ def run_reference(args, rank: int):
 
 
 # ---- GPU side ------------------------------------------------------------------------------------
+
+
+def _time(torch, stream, fn, reps: int = 5, warm: int = 2) -> float:
+    """Average seconds of fn() on the device (CUDA events on `stream`)."""
+    for _ in range(warm):
+        fn()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / reps
+
+
+def other_configs(torch, ofb, L, stream, peak):
+    """The uneven batch, the split-BF16 variant and the differentiable layer, each against the
+    plain FP32 GPU path on the same data (accuracy of each is checked by the test suite)."""
+    sptr = stream.cuda_stream
+    out = {}
+    g = torch.Generator(device="cuda").manual_seed(99)
+    # uneven batch: 20000 transforms, log2 n uniform in 4..16, packed, half inverse
+    rng = np.random.default_rng(0xC0F3)
+    log2n = rng.integers(4, 17, 20000).astype(np.int32)
+    inv = (rng.random(20000) < 0.5).astype(np.int32)
+    off = np.concatenate([[0], np.cumsum(1 << log2n.astype(np.int64))[:-1]])
+    ub = ofb.UnevenBatch(log2n, inv, off)
+    x = torch.rand(2 * ub.span, device="cuda", generator=g) * 2 - 1
+    y = torch.empty_like(x)
+    t_u = _time(torch, stream, lambda: ub.execute(x.data_ptr(), y.data_ptr(), sptr))
+    plans = {m: ofb.Plan(1 << m) for m in range(4, 17)}
+    base_in, base_out = x.data_ptr(), y.data_ptr()
+    calls = [((L.onefft_dev_inverse_batched if i else L.onefft_dev_forward_batched), plans[m].handle,
+              base_in + 8 * o, base_out + 8 * o) for m, i, o in zip(log2n.tolist(), inv.tolist(), off.tolist())]
+
+    def per_transform():
+        for f, h, a, b in calls:
+            f(h, a, b, 1, sptr)
+
+    t_p = _time(torch, stream, per_transform, reps=2, warm=1)
+    flops = float(sum(5.0 * (1 << m) * m for m in log2n.tolist()))
+    out["uneven 20000 x 2^(4..16)"] = {
+        "us_persistent": 1e6 * t_u, "us_per_transform_calls": 1e6 * t_p, "speedup": t_p / t_u,
+        "gflops": flops / t_u / 1e9, "gbs_16n": 16 * ub.span / t_u / 1e9, "frac_hbm": 16 * ub.span / t_u / 1e9 / peak,
+        "note": "one persistent launch vs one onefft_dev_*_batched call per transform (plain FP32 path); "
+                "results equal bit for bit except 2^13/2^14 (tests/test_gpu_uneven.py)"}
+    ub.destroy()
+    del x, y
+    # split-BF16 tensor-core variant vs plain FP32 on the same batches
+    for lg, batch in ((16, 256), (22, 16)):
+        n = 1 << lg
+        x = torch.randn(2 * n * batch, device="cuda", generator=g)
+        y = torch.empty_like(x)
+        tc, fp = ofb.Plan(n, bf16x3=True), ofb.Plan(n)
+        t_tc = _time(torch, stream, lambda: tc.dev_forward(x.data_ptr(), y.data_ptr(), batch, sptr))
+        t_fp = _time(torch, stream, lambda: fp.dev_forward(x.data_ptr(), y.data_ptr(), batch, sptr))
+        out[f"split-BF16 {batch} x 2^{lg}"] = {
+            "us_bf16x3": 1e6 * t_tc, "us_fp32": 1e6 * t_fp, "time_ratio_fp32_over_bf16x3": t_fp / t_tc,
+            "accepted": False,
+            "note": "rel RMS vs FP64 ~6.5e-6 against 1.5e-7 (FP32) on wide-range inputs: above the 2x bound, "
+                    "so no speedup at equal error exists (tests/test_gpu_bf16x3.py)"}
+        tc.destroy()
+        fp.destroy()
+        del x, y
+    # differentiable layer: forward + backward of sum |W * FFT(x)|^2, batch 512 x 8192
+    from onefft_b200 import torch_fft
+    n, batch = 8192, 512
+    xc = torch.randn(batch, n, dtype=torch.complex64, device="cuda", generator=g).requires_grad_(True)
+    wv = torch.rand(n, device="cuda", generator=g)
+
+    def step():
+        xc.grad = None
+        torch_fft.weighted_power_loss(xc, wv).backward()
+
+    t_s = _time(torch, stream, step)
+    t_f = _time(torch, stream, lambda: torch_fft._run("forward", xc.detach()))
+    out["autograd 512 x 8192"] = {"ms_fwd_bwd": 1e3 * t_s, "us_forward_kernel": 1e6 * t_f,
+                                  "note": "loss and gradient checked against FP64 finite differences and the "
+                                          "reference library (tests/test_gpu_autograd.py)"}
+    for p in plans.values():
+        p.destroy()
+    return out
 
 
 def main():
@@ -353,6 +437,14 @@ def main():
                         "pinned host buffers"}
         del host
 
+    # ---- the other configurations, measured beside the headline (rank 0, N = 1) ----
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        for w in work:  # free the headline buffers first
+            w["x"] = w["y"] = w["z"] = None
+        torch.cuda.empty_cache()
+        configs = other_configs(torch, ofb, L, stream, peak)
+
     # ---- CPU baseline: the reference library on this host (rank 0, N = 1) ----
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -372,7 +464,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": dict(WORKLOAD, parallelism=f"dp{world} (independent work per GPU, no collective)"),
                 "impl": "ours", "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
-                "gpu_launches": launches, "detail": detail}
+                "gpu_launches": launches, "detail": detail, "configs": configs}
         print(json.dumps(line), flush=True)
     for w in work:
         w["plan"].destroy()
