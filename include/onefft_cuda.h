@@ -45,6 +45,18 @@ ONEFFT_API int onefft_dev_inverse_batched(const onefft_plan *plan, const float *
 ONEFFT_API int onefft_dev_adjoint_batched(const onefft_plan *plan, const float *d_grad_out, float *d_grad_in, size_t batch,
                                void *stream);
 
+/* Loss and gradient of a weighted power spectrum in one pass over the data:
+ *   *d_loss = sum over the batch and k of w[k]^2 |(F x_b)[k]|^2          (double, on the device)
+ *   d_grad  = F^H (2 w^2 * F x_b) per transform (d loss / d conj(x), torch's convention; NULL =
+ *             loss only)
+ * with F the unnormalised forward transform of `plan` (FP32, 16 .. 2^14 points) and w a real
+ * weight vector of n floats shared by the batch. Each block keeps its transforms on chip from
+ * load to store: one read of x and one write of the gradient. The gradient equals the unfused
+ * computation (forward, elementwise 2 w^2 y, onefft_dev_adjoint_batched) bit for bit; d_loss is
+ * zeroed and accumulated by the call. OneFFT has no counterpart (it has no batch or loss API). */
+ONEFFT_API int onefft_dev_weighted_power_loss(const onefft_plan *plan, const float *d_x, const float *d_w,
+                                              float *d_grad, size_t batch, double *d_loss, void *stream);
+
 /* ---- batched transforms on host memory ---------------------------------------------------------
  * Same as calling onefft_plan_forward/_inverse on `batch` consecutive transforms of host (or
  * device) buffers, but pipelined: chunks are copied in, transformed and copied out on several

@@ -30,6 +30,7 @@ C_SYMBOLS = (
     "onefft_plan_create", "onefft_plan_destroy", "onefft_plan_forward", "onefft_plan_inverse",
     "onefft_plan_size", "onefft_implementation",
     "onefft_dev_forward_batched", "onefft_dev_inverse_batched", "onefft_dev_adjoint_batched",
+    "onefft_dev_weighted_power_loss",
     "onefft_plan_forward_batched", "onefft_plan_inverse_batched",
     "onefft_plan_create_split", "onefft_plan_create_tiles", "onefft_plan_create_bf16x3", "onefft_plan_passes",
     "onefft_uneven_create", "onefft_uneven_destroy", "onefft_uneven_span", "onefft_uneven_execute",
@@ -82,6 +83,8 @@ def lib() -> ctypes.CDLL:
         f = getattr(L, name)
         f.argtypes = [_vp, _vp, _vp, _sz, _vp]
         f.restype = ctypes.c_int
+    L.onefft_dev_weighted_power_loss.argtypes = [_vp, _vp, _vp, _vp, _sz, _vp, _vp]
+    L.onefft_dev_weighted_power_loss.restype = ctypes.c_int
     for name in ("onefft_plan_forward_batched", "onefft_plan_inverse_batched"):
         f = getattr(L, name)
         f.argtypes = [_vp, _vp, _vp, _sz]

@@ -46,6 +46,9 @@ cudaError_t launch_pass(int mode, int log_l, int log_c, const PassArgs& a, int b
 cudaError_t launch_single_kernel_tc(int log2n, const float2* in, float2* out, long long batch, const float2* stw,
                                     int inverse, cudaStream_t stream);
 cudaError_t launch_pass_tc(int mode, int log_l, const PassArgs& a, int batch, cudaStream_t stream);
+// fused forward -> sum w^2 |y|^2 -> adjoint of 2 w^2 y, n = 2^4 .. 2^14 (fft_fused.cu)
+cudaError_t launch_power_loss_grad(int log2n, const float2* x, const float* w, float2* grad, double* loss,
+                                   long long batch, const float2* stw, cudaStream_t stream);
 cudaError_t launch_stage_table(float2* dst, int log_l, cudaStream_t stream);
 cudaError_t launch_big_table(double2* lo, double2* hi, int log2n, int lo_bits, cudaStream_t stream);
 int stage_table_entries_host(int log_l);

@@ -471,6 +471,28 @@ extern "C" int onefft_dev_adjoint_batched(const onefft_plan *plan, const float *
     return dev_batched(plan, d_grad_out, d_grad_in, batch, 1, stream);
 }
 
+extern "C" int onefft_dev_weighted_power_loss(const onefft_plan *plan, const float *d_x, const float *d_w,
+                                              float *d_grad, size_t batch, double *d_loss, void *stream) {
+    t_last_error.clear();
+    if (!plan) return set_error(ONEFFT_ERR_ARG, "NULL plan");
+    if (plan->npass != 1 || plan->tc || plan->log2n < 4)
+        return set_error(ONEFFT_ERR_ARG, "the fused loss needs an FP32 plan of 16 .. 2^14 points");
+    if (!d_x || !d_w || !d_loss || batch == 0) return set_error(ONEFFT_ERR_ARG, "NULL buffer or empty batch");
+    if ((((uintptr_t)d_x | (uintptr_t)d_grad | (uintptr_t)d_loss) & 7) || ((uintptr_t)d_w & 3))
+        return set_error(ONEFFT_ERR_ARG, "misaligned device buffer");
+    if (batch > ((size_t)1 << 40) / plan->n) return set_error(ONEFFT_ERR_ARG, "batch too large");
+    if (d_grad && ranges_overlap(d_x, d_grad, batch * plan->n * sizeof(float2)))
+        return set_error(ONEFFT_ERR_ARG, "input and gradient overlap");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaMemsetAsync(d_loss, 0, sizeof(double), s);
+    if (e == cudaSuccess) {
+        g_launches.fetch_add(1);
+        e = launch_power_loss_grad(plan->log2n, (const float2 *)d_x, d_w, (float2 *)d_grad, d_loss, (long long)batch,
+                                   plan->stw[0], s);
+    }
+    return e == cudaSuccess ? 0 : cuda_error(e, "fused loss launch");
+}
+
 // ---- per-thread host staging -------------------------------------------------------------------
 
 namespace {

@@ -100,3 +100,37 @@ def weighted_power_loss(x: torch.Tensor, w: torch.Tensor) -> torch.Tensor:
     """sum over the batch and frequencies of |w * fft(x)|^2, w real of length n."""
     y = fft(x)
     return (torch.view_as_real(y).square().sum(-1) * w.square()).sum()
+
+
+class _FusedPowerLoss(torch.autograd.Function):
+    """Loss and gradient from one kernel pass (onefft_dev_weighted_power_loss): the gradient is
+    computed with the loss and kept until backward."""
+
+    @staticmethod
+    def forward(ctx, x, w):
+        x = _check(x)
+        w = w.detach().to(torch.float32).contiguous()
+        n = x.shape[-1]
+        batch = x.numel() // n
+        plan = _plan(n, x.device.index)
+        grad = torch.empty_like(x) if x.requires_grad else None
+        loss = torch.empty((), dtype=torch.float64, device=x.device)
+        stream = torch.cuda.current_stream(x.device).cuda_stream
+        with torch.cuda.device(x.device):
+            rc = lib().onefft_dev_weighted_power_loss(plan.handle, x.data_ptr(), w.data_ptr(),
+                                                       grad.data_ptr() if grad is not None else None, batch,
+                                                       loss.data_ptr(), stream)
+        if rc != 0:
+            raise RuntimeError(f"onefft fused loss failed ({rc}): {last_error()}")
+        ctx.save_for_backward(grad if grad is not None else torch.empty(0))
+        return loss.to(torch.float32)
+
+    @staticmethod
+    def backward(ctx, g):
+        (grad,) = ctx.saved_tensors
+        return grad * g.to(grad.real.dtype), None
+
+
+def weighted_power_loss_fused(x: torch.Tensor, w: torch.Tensor) -> torch.Tensor:
+    """Same value and gradient as weighted_power_loss, from a single fused kernel."""
+    return _FusedPowerLoss.apply(x, w)

@@ -85,6 +85,32 @@ def test_gradient_vs_reference_library(ofb, oracle, data):
         assert d_ours <= 2 * d_ref + 1e-9, (r, d_ours, d_ref)
 
 
+def test_fused_loss_equals_unfused(ofb, data):
+    """The one-kernel loss + gradient gives the unfused path's gradient bit for bit and its loss
+    up to summation order."""
+    T = torch()
+    from onefft_b200 import torch_fft
+    x, w = data
+    wt = T.from_numpy(w).cuda()
+    xa = T.from_numpy(x.copy()).cuda().requires_grad_(True)
+    la = torch_fft.weighted_power_loss(xa, wt)
+    la.backward()
+    xb = T.from_numpy(x.copy()).cuda().requires_grad_(True)
+    lb = torch_fft.weighted_power_loss_fused(xb, wt)
+    lb.backward()
+    assert abs(la.item() - lb.item()) / la.item() < 1e-5
+    assert T.equal(T.view_as_real(xa.grad), T.view_as_real(xb.grad))
+    # other sizes of the fused kernel (one-kernel range), loss against FP64
+    for lg in (4, 7, 10, 13, 14):
+        n = 1 << lg
+        xs = T.randn(8, n, dtype=T.complex64, device="cuda")
+        ws = T.rand(n, device="cuda")
+        lf = torch_fft.weighted_power_loss_fused(xs, ws).item()
+        l64 = (np.abs(np.fft.fft(xs.cpu().numpy().astype(np.complex128), axis=-1)) ** 2
+               * ws.cpu().numpy().astype(np.float64) ** 2).sum()
+        assert abs(lf - l64) / l64 < 1e-5, (lg, lf, l64)
+
+
 def test_adjoint_identity_and_inverse_grad(ofb, oracle):
     T = torch()
     from onefft_b200 import torch_fft
