@@ -75,6 +75,57 @@ def test_two_ranks_shard_and_reduce(oracle):
     assert results[0][2] == results[1][2]
 
 
+def _numpy_fft_last_dim(t):
+    """CPU stand-in for the GPU kernels: FP64 FFT along the last dimension, back to complex64."""
+    import torch
+    return torch.from_numpy(np.fft.fft(t.numpy().astype(np.complex128), axis=-1).astype(np.complex64))
+
+
+def dist_worker(rank: int, world: int, port: int, n1: int, n2: int, q):
+    import torch
+    import torch.distributed as dist
+
+    from onefft_b200.distributed import dist_fft
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        rng = np.random.default_rng(42)
+        x = (rng.standard_normal(n1 * n2) + 1j * rng.standard_normal(n1 * n2)).astype(np.complex64)
+        c2 = n2 // world
+        cols = torch.from_numpy(np.ascontiguousarray(x.reshape(n1, n2)[:, rank * c2:(rank + 1) * c2]))
+        out = dist_fft(cols, n1, n2, fft_last_dim=_numpy_fft_last_dim)
+        q.put((rank, out.numpy()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_distributed_four_step_one_all_to_all(world):
+    n1, n2 = 64, 128
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=dist_worker, args=(r, world, port, n1, n2, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    rng = np.random.default_rng(42)
+    x = (rng.standard_normal(n1 * n2) + 1j * rng.standard_normal(n1 * n2)).astype(np.complex64)
+    want = np.fft.fft(x.astype(np.complex128))
+    r1 = n1 // world
+    for rank, blk in res.items():
+        # block element [k1 - rank r1][k2] = X[k1 + n1 k2]
+        k1 = np.arange(rank * r1, (rank + 1) * r1)[:, None]
+        k2 = np.arange(n2)[None, :]
+        ref = want[k1 + n1 * k2]
+        assert np.linalg.norm(blk - ref) / np.linalg.norm(ref) < 1e-6
+
+
 def test_shard_balance():
     from onefft_b200.shard import shard_batch, shard_uneven, transform_cost
     assert [shard_batch(10, 3, r) for r in range(3)] == [(0, 4), (4, 3), (7, 3)]
