@@ -19,9 +19,9 @@ __device__ __forceinline__ double2 big_twiddle_f64(const double2* __restrict__ l
     return zmul(__ldg(lo + (t & ((1u << lo_bits) - 1))), __ldg(hi + (t >> lo_bits)));
 }
 
-// L2 cache hints: the input of a transform is read exactly once (evict first); the intermediate
-// array between passes may be kept in L2 for the next pass (evict last).
-__device__ __forceinline__ float2 ld_stream(const float2* p) { return __ldcs(p); }
+// Loads of data the kernel never writes go through the read-only path; the intermediate array
+// between passes may be kept in L2 for the next pass (evict last).
+__device__ __forceinline__ float2 ld_stream(const float2* p) { return __ldg(p); }
 __device__ __forceinline__ unsigned long long policy_evict_last() {
     unsigned long long pol;
     asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));

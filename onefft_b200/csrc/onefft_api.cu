@@ -124,7 +124,7 @@ static const Shape kTuned[] = {
     /* 21 */ {2, {11, 10, 0}, {3, 4, 0}, 1, 0},
     /* 22 */ {3, {7, 7, 8}, {4, 4, 4}, 1, 0},
     /* 23 */ {3, {8, 8, 7}, {3, 3, 4}, 0, 0},
-    /* 24 */ {3, {8, 8, 8}, {4, 4, 4}, 0, 0},
+    /* 24 */ {3, {8, 8, 8}, {4, 4, 4}, 1, 0},
     /* 25 */ {3, {8, 9, 8}, {4, 3, 4}, 0, 0},
     /* 26 */ {3, {8, 9, 9}, {4, 3, 4}, 1, 0},
     /* 27 */ {3, {9, 9, 9}, {4, 3, 4}, 1, 0},

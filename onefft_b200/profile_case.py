@@ -25,6 +25,7 @@ def main():
     ap.add_argument("--batch", type=int, default=1)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--inverse", action="store_true")
+    ap.add_argument("--chunk", type=int, default=0, help="three passes: log2 last-digit columns per chunk")
     ap.add_argument("--uneven", type=int, default=0, help="run an uneven batch of this many transforms")
     args = ap.parse_args()
     g = torch.Generator(device="cuda").manual_seed(7)
@@ -44,7 +45,7 @@ def main():
     n = 1 << args.log2n
     split = tuple(int(v) for v in args.split.split(",")) if args.split else None
     cols = tuple(int(v) for v in args.cols.split(",")) if args.cols else None
-    plan = ofb.Plan(n, split=split, cols=cols)
+    plan = ofb.Plan(n, split=split, cols=cols, chunk=args.chunk)
     x = torch.randn(2 * n * args.batch, device="cuda", generator=g)
     y = torch.empty_like(x)
     f = plan.dev_inverse if args.inverse else plan.dev_forward
