@@ -73,13 +73,16 @@ ONEFFT_API int onefft_plan_inverse_batched(const onefft_plan *plan, const float 
 ONEFFT_API onefft_plan *onefft_plan_create_split(size_t n, int npass, const int *log2_len);
 
 /* As onefft_plan_create_split, also choosing each pass's tile width: 2^log2_cols[p] adjacent
- * columns per thread block (2 .. 4, at most 16384 values per tile; NULL = default widths),
- * whether the array between passes is stored with L2 evict-last priority (l2_keep != 0), and,
- * for three passes, log2_chunk > 0 to run the first two passes chunk by chunk over 2^log2_chunk
- * columns of the last digit so that each chunk's intermediate values stay in L2 (0 = whole
- * passes). */
+ * columns per thread block (1 .. 4, at most 16384 values per tile; NULL = default widths),
+ * `options` (ONEFFT_OPT_L2_KEEP: store the array between passes with L2 evict-last priority;
+ * ONEFFT_OPT_TMA: stage each pass tile through one bulk tensor copy where the tile shape has
+ * such a kernel and the buffers are 16-byte aligned), and, for three passes, log2_chunk > 0 to
+ * run the first two passes chunk by chunk over 2^log2_chunk columns of the last digit so that
+ * each chunk's intermediate values stay in L2 (0 = whole passes). */
+#define ONEFFT_OPT_L2_KEEP 1
+#define ONEFFT_OPT_TMA 2
 ONEFFT_API onefft_plan *onefft_plan_create_tiles(size_t n, int npass, const int *log2_len, const int *log2_cols,
-                                                 int l2_keep, int log2_chunk);
+                                                 int options, int log2_chunk);
 
 /* ---- split-BF16 tensor-core variant --------------------------------------------------------------
  * A plan whose radix-16 stages run as dense complex 16x16 matrix products on the tensor cores:

@@ -171,7 +171,8 @@ class Plan:
     """Owns the device tables of one size (OneFFT's onefft::Plan, include/onefft.h:136-167)."""
 
     def __init__(self, n: int, split: tuple[int, ...] | None = None, cols: tuple[int, ...] | None = None,
-                 l2_keep: bool = True, chunk: int = 0, bf16x3: bool = False, require_accepted: bool = False):
+                 l2_keep: bool = True, chunk: int = 0, bf16x3: bool = False, require_accepted: bool = False,
+                 tma: bool = False):
         """split: log2 pass lengths (None = tuned table); cols: log2 tile widths per pass;
         chunk: three passes only, log2 last-digit columns per L2-resident chunk (0 = none);
         bf16x3: the split-BF16 tensor-core variant (require_accepted: only at sizes where it
@@ -184,7 +185,8 @@ class Plan:
         else:
             arr = (ctypes.c_int * len(split))(*split)
             carr = (ctypes.c_int * len(split))(*cols) if cols is not None else None
-            h = L.onefft_plan_create_tiles(n, len(split), arr, carr, int(l2_keep), int(chunk))
+            options = (1 if l2_keep else 0) | (2 if tma else 0)  # ONEFFT_OPT_L2_KEEP | ONEFFT_OPT_TMA
+            h = L.onefft_plan_create_tiles(n, len(split), arr, carr, options, int(chunk))
         if not h:
             raise ValueError(f"no plan for n={n}: {last_error()}")
         self._h = h

@@ -24,6 +24,13 @@ def tile_ok(l: int, c: int) -> bool:
     return 4 <= l <= 12 and c <= 4 and l + c <= 14 and (c >= 2 or (c == 1 and l >= 10))
 
 
+def tma_ok(l: int, c: int) -> bool:
+    """Tile shapes with a bulk-tensor-copy kernel (fft_tma.cu, pass_tma_supported)."""
+    return 6 <= l <= 12 and 1 <= c <= 4 and l + c <= 13 and (l, c) in {
+        (12, 1), (11, 1), (11, 2), (10, 1), (10, 2), (10, 3), (9, 2), (9, 3), (9, 4), (8, 2), (8, 3), (8, 4),
+        (7, 3), (7, 4), (6, 4)}
+
+
 def candidates(m: int):
     """(log2 lengths, log2 tile widths, log2 chunk) shapes worth timing for 2^m."""
     out = []
@@ -87,10 +94,12 @@ def main():
         best = None
         rows = []
         cands = candidates(m)[: args.max_candidates]
-        for ls, cs, g in cands:
-            for keep in (True, False):
+        variants = [(ls, cs, g, keep, tma) for ls, cs, g in cands for keep in (True, False)
+                    for tma in ((False, True) if any(tma_ok(l, c) for l, c in zip(ls, cs)) else (False,))]
+        for ls, cs, g, keep, tma in variants:
+            if True:
                 try:
-                    p = ofb.Plan(n, split=ls, cols=cs, l2_keep=keep, chunk=g)
+                    p = ofb.Plan(n, split=ls, cols=cs, l2_keep=keep, chunk=g, tma=tma)
                 except ValueError:
                     continue
                 y.zero_()
@@ -104,7 +113,7 @@ def main():
                     continue
                 us = time_plan(p, x, y, args.reps, flush)
                 p.destroy()
-                rows.append({"len": ls, "cols": cs, "l2_keep": keep, "chunk": g, "us": us,
+                rows.append({"len": ls, "cols": cs, "l2_keep": keep, "chunk": g, "tma": tma, "us": us,
                              "gbs_16n": 16 * n / us / 1e3})
                 if best is None or us < best["us"]:
                     best = rows[-1]
@@ -112,16 +121,17 @@ def main():
         ref.destroy()
         results[m] = {"best": best, "default_us": base_us, "all": sorted(rows, key=lambda r: r["us"])[:10]}
         print(f"m={m}: best {best['len']} cols {best['cols']} chunk {best['chunk']} keep={best['l2_keep']} "
-              f"{best['us']:.1f} us ({best['gbs_16n']:.0f} GB/s of 16n); default {base_us:.1f} us", flush=True)
+              f"tma={best['tma']} {best['us']:.1f} us ({best['gbs_16n']:.0f} GB/s of 16n); default {base_us:.1f} us",
+              flush=True)
         del x, y, want
         torch.cuda.empty_cache()
-    print("// tuned shapes: {npass, {len}, {cols}, l2_keep, chunk} for log2 n =", args.min, "..", args.max)
+    print("// tuned shapes: {npass, {len}, {cols}, l2_keep, chunk, tma} for log2 n =", args.min, "..", args.max)
     for m, r in results.items():
         b = r["best"]
         ls = list(b["len"]) + [0] * (3 - len(b["len"]))
         cs = list(b["cols"]) + [0] * (3 - len(b["cols"]))
         print(f"    /* {m} */ {{{len(b['len'])}, {{{ls[0]}, {ls[1]}, {ls[2]}}}, {{{cs[0]}, {cs[1]}, {cs[2]}}}, "
-              f"{int(b['l2_keep'])}, {b['chunk']}}},")
+              f"{int(b['l2_keep'])}, {b['chunk']}, {int(b['tma'])}}},")
     if args.out:
         with open(args.out, "w") as f:
             json.dump(results, f, indent=1)

@@ -29,6 +29,7 @@ struct PassArgs {
     unsigned outer_base;
     unsigned inner_base;
     unsigned ntiles;  // grid size of the launch (tiles per transform)
+    unsigned* err;    // plan's error word: set by a kernel whose bounded wait ran out
 };
 
 // Largest size handled by one kernel (k_tiny / k_batched).
@@ -41,6 +42,10 @@ bool pass_tile_supported(int log_l, int log_c);
 cudaError_t launch_single_kernel(int log2n, const float2* in, float2* out, long long batch, const float2* stw,
                                  int inverse, cudaStream_t stream);
 cudaError_t launch_pass(int mode, int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t stream);
+// TMA-staged passes (fft_tma.cu): same arithmetic as launch_pass; 16-byte aligned buffers,
+// batch <= 65535, shapes pass_tma_supported()
+bool pass_tma_supported(int log_l, int log_c);
+cudaError_t launch_pass_tma(int mode, int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t stream);
 // split-BF16 tensor-core variants (fft_tc.cu): n = 2^4 .. 2^14 in one kernel; pass lengths
 // 2^5 .. 2^12 with the default tile width pass_log_c()
 cudaError_t launch_single_kernel_tc(int log2n, const float2* in, float2* out, long long batch, const float2* stw,

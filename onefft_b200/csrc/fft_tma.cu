@@ -1,0 +1,275 @@
+// TMA-staged pass kernels (sm_100a): the tile of a pass — C adjacent columns of L values at a
+// stride of S complex values — arrives in shared memory through ONE cp.async.bulk.tensor copy
+// (a 4-D/5-D box over the strided array) instead of C*L/2 narrow strided loads, and the strided
+// in-place passes write their tile back with one bulk tensor store. The arithmetic is the FP32
+// tile engine of k_pass (fft_tiles.cuh), so results equal k_pass bit for bit.
+//
+// Why: with narrow tiles (C = 2 .. 8) every warp load touches many 8..64-byte row segments; the
+// load/store unit and MIO queues saturate long before HBM does (ncu: lg/mio throttle stalls,
+// 22-32 % issue active on the 2^12-point passes). The copy engine moves the same box with no
+// per-thread address work.
+//
+// Waits on the mbarrier are bounded: if a copy does not complete within the limit, the kernel
+// records the failure in the plan's error word, waits once more (bounded) and returns without
+// touching global memory; host calls that synchronise report it.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "fft_tiles.cuh"
+
+namespace ofb {
+
+constexpr unsigned kWaitLimit = 1u << 22;  // try_wait polls (each may suspend briefly): ~0.1-1 s
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned phase) {
+    const unsigned a = smem_u32(bar);
+    for (unsigned i = 0; i < kWaitLimit; ++i) {
+        unsigned ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(phase)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"((unsigned long long)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3, int c4,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5, %6}], [%7];" ::"r"(smem_u32(dst)),
+        "l"((unsigned long long)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_store_5d(const CUtensorMap* map, const void* src, int c0, int c1, int c2, int c3,
+                                             int c4) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4, %5, %6}], [%1];" ::"l"(
+            (unsigned long long)map),
+        "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
+        : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// One tile per block; MODE as k_pass. `tin` maps the pass's input, `tout` its output (MODE 1/2:
+// the same array, in place). Shared memory: the tile (dense as the copy lands, then reused
+// padded by the exchanges), the inter-pass twiddle factors, the mbarrier.
+template <int LOG_L, int LOG_C, int MODE>
+__global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4))
+    k_pass_tma(PassArgs a, const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout) {
+    constexpr int L = 1 << LOG_L, T = L / 16, C = 1 << LOG_C;
+    constexpr int ELO = L < 256 ? L : 256;
+    extern __shared__ __align__(1024) float2 smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + spad(C * L - 1) + 1 + 17 * C + 1);
+    const int tid = threadIdx.x;
+    const int c = tid & (C - 1);
+    const int j = tid >> LOG_C;
+    const unsigned t = blockIdx.x;
+    const int b = blockIdx.y;
+    const unsigned col0 = a.tli >= 31 ? (t << LOG_C)
+                                      : ((a.outer_base + (t >> a.tli)) << a.outer_shift) + a.inner_base +
+                                            ((t & ((1u << a.tli) - 1)) << LOG_C);
+    const int q0 = (int)(col0 & ((1u << a.log_s) - 1)), h = (int)(col0 >> a.log_s);
+    if (smem_u32(smem) & 127) {  // bulk tensor copies need a 128-byte aligned destination
+        if (tid == 0) atomicExch(a.err, 2u);
+        return;
+    }
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        mbar_expect_tx(bar, (unsigned)(C * L * sizeof(float2)));
+        if (MODE == 0) tma_load_4d(smem, &tin, (int)col0, 0, 0, b, bar);
+        else tma_load_5d(smem, &tin, q0, 0, 0, h, b, bar);
+    }
+    (void)ELO;
+    // inter-pass twiddle factors (as pass_tile) while the copy is in flight
+    float2* tws = smem + spad(C * L - 1) + 1;
+    if (MODE != 2) {
+        const unsigned hs = (col0 >> a.log_s) << a.log_s;
+        for (int i = tid; i < (MODE == 0 ? C : 1) * 16; i += C * T) {
+            const int cc = i >> 4, kk = i & 15;
+            const unsigned f = MODE == 0 ? col0 + cc : hs;
+            double2 w = big_twiddle_f64(a.tw_lo, a.tw_hi, a.lo_bits, f * (unsigned)T * (unsigned)kk);
+            tws[cc * 17 + kk] = make_float2((float)w.x, (float)w.y);
+        }
+    }
+    __syncthreads();  // the barrier is initialised before anyone waits on it
+    const bool ok = mbar_wait(bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+            atomicExch(a.err, 1u);
+            mbar_wait(bar, 0);  // let a late copy land before the block's memory is released
+        }
+        return;
+    }
+    float2 v[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        float2 x = smem[(j + T * k) * C + c];
+        v[k] = a.swap_in ? swap_ri(x) : x;
+    }
+    __syncthreads();  // the dense tile is consumed; the exchanges reuse its memory
+    tile_fft<LOG_L, C>(v, j, a.stw, smem, c);
+    if (MODE != 2) {
+        if (Stages<LOG_L>::COUNT == 1) __syncthreads();
+        const unsigned f = MODE == 0 ? col0 + c : (col0 >> a.log_s) << a.log_s;
+        const double2 wj = big_twiddle_f64(a.tw_lo, a.tw_hi, a.lo_bits, f * (unsigned)j);
+        const float2 wjf = make_float2((float)wj.x, (float)wj.y);
+        const float2* tw = tws + (MODE == 0 ? c * 17 : 0);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[k] = cmul(v[k], cmul(wjf, tw[k]));
+    }
+    if (MODE == 0) {
+        // contiguous column runs at their digit-reversed place, as k_pass
+        {
+            float2* w = smem + spad(j * C + c);
+#pragma unroll
+            for (int k = 0; k < 16; ++k) w[padc(k * T * C)] = v[k];
+        }
+        __syncthreads();
+        const int cc = tid >> (LOG_L - 4), kk0 = tid & (T - 1);
+        const unsigned rr = col0 + cc;
+        const unsigned j2 = rr & ((1u << a.rev_b2) - 1), j1 = rr >> a.rev_b2;
+        float2* q = a.out + ((long long)b << a.log2n) + (((j1 + (j2 << a.rev_b1)) << LOG_L) + kk0);
+        const float2* r = smem + spad(kk0 * C + cc);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) q[i * T] = r[padc(i * T * C)];
+    } else {
+        // dense tile back in shared memory, then one bulk tensor store
+#pragma unroll
+        for (int k = 0; k < 16; ++k) smem[(j + T * k) * C + c] = a.swap_out ? swap_ri(v[k]) : v[k];
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) tma_store_5d(&tout, smem, q0, 0, 0, h, b);
+    }
+}
+
+// ---- host side ----------------------------------------------------------------------------------
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+
+// Tensor map of the pass tile: MODE 0 {column r, row-in-box, row-box, batch} over `in`;
+// MODE 1/2 {q, row-in-box, row-box, h, batch} over `out`. 8-byte elements, no swizzle.
+static bool make_map(CUtensorMap* m, const float2* base, int mode, int log2n, int log_l, int log_c, int log_s,
+                     int batch) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+    if (!enc) return false;
+    const cuuint64_t n = 1ull << log2n, L = 1ull << log_l, elo = L < 256 ? L : 256, ehi = L / elo;
+    cuuint64_t dims[5], strides[4];
+    cuuint32_t box[5], estr[5] = {1, 1, 1, 1, 1};
+    int rank;
+    if (mode == 0) {
+        const cuuint64_t cols = n >> log_l;
+        dims[0] = cols, dims[1] = elo, dims[2] = ehi, dims[3] = (cuuint64_t)batch;
+        strides[0] = cols * 8, strides[1] = elo * cols * 8, strides[2] = n * 8;
+        box[0] = 1u << log_c, box[1] = (cuuint32_t)elo, box[2] = (cuuint32_t)ehi, box[3] = 1;
+        rank = 4;
+    } else {
+        const cuuint64_t S = 1ull << log_s, H = n >> (log_s + log_l);
+        dims[0] = S, dims[1] = elo, dims[2] = ehi, dims[3] = H, dims[4] = (cuuint64_t)batch;
+        strides[0] = S * 8, strides[1] = elo * S * 8, strides[2] = L * S * 8, strides[3] = n * 8;
+        box[0] = 1u << log_c, box[1] = (cuuint32_t)elo, box[2] = (cuuint32_t)ehi, box[3] = 1, box[4] = 1;
+        rank = 5;
+    }
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (cuuint32_t)rank, (void*)base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+template <int LOG_L, int LOG_C, int MODE>
+static cudaError_t launch_tma_t(const PassArgs& a, int batch, cudaStream_t stream) {
+    constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
+    constexpr int SMEM = smem_bytes(LOG_L, LOG_C) + (int)sizeof(float2) * (17 * (1 << LOG_C) + 2) + 16;
+    auto kernel = k_pass_tma<LOG_L, LOG_C, MODE>;
+    static cudaError_t attr =
+        SMEM > 48 * 1024 ? cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) : cudaSuccess;
+    if (attr != cudaSuccess) return attr;
+    // MODE 0 loads from `in` and stores with plain coalesced stores (tout unused); MODE 1/2
+    // load and store the same tile of `out`
+    CUtensorMap tin;
+    if (!make_map(&tin, MODE == 0 ? a.in : a.out, MODE, a.log2n, LOG_L, LOG_C, a.log_s, batch))
+        return cudaErrorInvalidValue;
+    const CUtensorMap& tout = tin;
+    dim3 grid(a.ntiles ? a.ntiles : 1u << (a.log2n - LOG_L - LOG_C), (unsigned)batch, 1);
+    PassArgs b = a;
+    if (!a.ntiles) b.tli = 31;
+    kernel<<<grid, THREADS, SMEM, stream>>>(b, tin, tout);
+    return cudaGetLastError();
+}
+
+// Tile shapes with a TMA kernel: widths 2 .. 16 columns (16-byte minimum row segment), up to
+// 8192 values per tile.
+bool pass_tma_supported(int log_l, int log_c) {
+    return log_l >= 6 && log_l <= 12 && log_c >= 1 && log_c <= 4 && log_l + log_c <= 13;
+}
+
+template <int MODE>
+static cudaError_t launch_tma_mode(int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t s) {
+#define OFB_TMA_CASE(LL, LC) \
+    if (log_l == LL && log_c == LC) return launch_tma_t<LL, LC, MODE>(a, batch, s);
+    OFB_TMA_CASE(12, 1)
+    OFB_TMA_CASE(11, 1)
+    OFB_TMA_CASE(11, 2)
+    OFB_TMA_CASE(10, 1)
+    OFB_TMA_CASE(10, 2)
+    OFB_TMA_CASE(10, 3)
+    OFB_TMA_CASE(9, 2)
+    OFB_TMA_CASE(9, 3)
+    OFB_TMA_CASE(9, 4)
+    OFB_TMA_CASE(8, 2)
+    OFB_TMA_CASE(8, 3)
+    OFB_TMA_CASE(8, 4)
+    OFB_TMA_CASE(7, 3)
+    OFB_TMA_CASE(7, 4)
+    OFB_TMA_CASE(6, 4)
+#undef OFB_TMA_CASE
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_pass_tma(int mode, int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t stream) {
+    if (!pass_tma_supported(log_l, log_c) || batch > 65535) return cudaErrorInvalidValue;
+    switch (mode) {
+    case 0: return launch_tma_mode<0>(log_l, log_c, a, batch, stream);
+    case 1: return launch_tma_mode<1>(log_l, log_c, a, batch, stream);
+    default: return launch_tma_mode<2>(log_l, log_c, a, batch, stream);
+    }
+}
+
+}  // namespace ofb

@@ -93,6 +93,8 @@ struct onefft_plan {
     int l2_keep;           // intermediate stores with L2 evict-last priority
     int chunk;             // three passes: log2 of the last-digit columns per chunk of passes 0+1 (0 = none)
     int tc;                // radix-16 stages as split-BF16 tensor-core products (onefft_plan_create_bf16x3)
+    int tma;               // passes staged through bulk tensor copies where the tile shape has a TMA kernel
+    unsigned *err;         // device word: set by a kernel whose bounded wait ran out
     void *mem;             // the one device allocation
     size_t mem_bytes;
     const float2 *stw[3];  // stage twiddles of each pass's length
@@ -110,24 +112,27 @@ struct Shape {
     int cols[3];
     int l2_keep;
     int chunk;
+    int tma;
 };
 
 // Fastest shapes measured on a B200 by onefft_b200/autotune.py (forward transform, L2 flushed
-// before each repetition): {npass, {log2 lengths}, {log2 tile widths}, l2_keep, chunk}.
+// before each repetition): {npass, {log2 lengths}, {log2 tile widths}, l2_keep, chunk, tma}.
+// 2^16 keeps the (8, 8) split (as fast as the best) so the uneven batch's in-block passes,
+// which use it, stay bit-identical to this path.
 static const Shape kTuned[] = {
-    /* 15 */ {2, {8, 7, 0}, {3, 4, 0}, 1, 0},
-    /* 16 */ {2, {8, 8, 0}, {3, 3, 0}, 1, 0},
-    /* 17 */ {2, {9, 8, 0}, {2, 3, 0}, 1, 0},
-    /* 18 */ {2, {8, 10, 0}, {4, 2, 0}, 1, 0},
-    /* 19 */ {2, {8, 11, 0}, {4, 2, 0}, 0, 0},
-    /* 20 */ {2, {10, 10, 0}, {2, 3, 0}, 0, 0},
-    /* 21 */ {2, {11, 10, 0}, {3, 4, 0}, 1, 0},
-    /* 22 */ {3, {7, 7, 8}, {4, 4, 4}, 1, 0},
-    /* 23 */ {3, {8, 8, 7}, {3, 3, 4}, 0, 0},
-    /* 24 */ {3, {8, 8, 8}, {4, 4, 4}, 1, 0},
-    /* 25 */ {3, {8, 9, 8}, {4, 3, 4}, 0, 0},
-    /* 26 */ {3, {8, 9, 9}, {4, 3, 4}, 1, 0},
-    /* 27 */ {3, {9, 9, 9}, {4, 3, 4}, 1, 0},
+    /* 15 */ {2, {8, 7, 0}, {3, 4, 0}, 1, 0, 1},
+    /* 16 */ {2, {8, 8, 0}, {3, 3, 0}, 1, 0, 1},
+    /* 17 */ {2, {10, 7, 0}, {1, 4, 0}, 0, 0, 0},
+    /* 18 */ {2, {10, 8, 0}, {2, 3, 0}, 0, 0, 0},
+    /* 19 */ {2, {8, 11, 0}, {4, 1, 0}, 1, 0, 0},
+    /* 20 */ {2, {11, 9, 0}, {1, 4, 0}, 1, 0, 1},
+    /* 21 */ {2, {11, 10, 0}, {2, 3, 0}, 1, 0, 0},
+    /* 22 */ {3, {8, 7, 7}, {3, 4, 4}, 1, 0, 1},
+    /* 23 */ {3, {8, 8, 7}, {3, 4, 4}, 1, 0, 1},
+    /* 24 */ {3, {8, 8, 8}, {3, 3, 3}, 0, 0, 1},
+    /* 25 */ {3, {8, 8, 9}, {3, 3, 3}, 1, 0, 1},
+    /* 26 */ {3, {8, 9, 9}, {3, 3, 3}, 1, 0, 1},
+    /* 27 */ {3, {8, 9, 10}, {4, 3, 3}, 1, 0, 1},
 };
 
 static Shape tuned_shape(int m) {
@@ -150,6 +155,7 @@ static Shape tuned_shape(int m) {
     }
     for (int i = 0; i < s.npass; ++i) s.cols[i] = pass_log_c(s.len[i]);
     s.l2_keep = 1;
+    s.tma = 1;  // passes whose tile shape has a TMA kernel use it (as the tuned large sizes do)
     return s;
 }
 
@@ -188,6 +194,7 @@ static onefft_plan *plan_build(size_t n, int m, const Shape &shape) {
     p->npass = shape.npass;
     p->l2_keep = shape.l2_keep;
     p->chunk = shape.chunk;
+    p->tma = shape.tma;
     for (int i = 0; i < shape.npass; ++i) {
         p->len[i] = shape.len[i];
         p->cols[i] = shape.cols[i];
@@ -206,7 +213,8 @@ static onefft_plan *plan_build(size_t n, int m, const Shape &shape) {
         hi_off = bytes;
         bytes = align256(bytes + sizeof(double2) * ((size_t)1 << (m - p->lo_bits)));
     }
-    if (bytes == 0) bytes = 256;
+    const size_t err_off = bytes;  // the error word
+    bytes += 256;
     e = dev_alloc(&p->mem, bytes);
     if (e != cudaSuccess) {
         delete p;
@@ -216,8 +224,10 @@ static onefft_plan *plan_build(size_t n, int m, const Shape &shape) {
     }
     p->mem_bytes = bytes;
     char *base = (char *)p->mem;
+    p->err = (unsigned *)(base + err_off);
     cudaStream_t s;
     e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMemsetAsync(p->err, 0, sizeof(unsigned), s);
     if (e == cudaSuccess) {
         for (int i = 0; i < p->npass && e == cudaSuccess; ++i) {
             p->stw[i] = (const float2 *)(base + off[i]);
@@ -251,7 +261,7 @@ extern "C" onefft_plan *onefft_plan_create(size_t n) {
 }
 
 extern "C" onefft_plan *onefft_plan_create_tiles(size_t n, int npass, const int *log2_len, const int *log2_cols,
-                                                 int l2_keep, int log2_chunk) {
+                                                 int options, int log2_chunk) {
     int m;
     if (!size_log2(n, &m)) {
         set_error(ONEFFT_ERR_SIZE, "n=%zu is not a power of two in [1, 2^30]", n);
@@ -263,7 +273,8 @@ extern "C" onefft_plan *onefft_plan_create_tiles(size_t n, int npass, const int 
     }
     Shape s{};
     s.npass = npass;
-    s.l2_keep = l2_keep ? 1 : 0;
+    s.l2_keep = (options & ONEFFT_OPT_L2_KEEP) ? 1 : 0;
+    s.tma = (options & ONEFFT_OPT_TMA) ? 1 : 0;
     s.chunk = log2_chunk > 0 ? log2_chunk : 0;
     for (int i = 0; i < npass; ++i) {
         s.len[i] = log2_len[i];
@@ -294,6 +305,7 @@ extern "C" onefft_plan *onefft_plan_create_bf16x3(size_t n, int require_accepted
     }
     Shape s = tuned_shape(m);
     s.chunk = 0;
+    s.tma = 0;
     for (int i = 0; i < s.npass; ++i) {
         s.cols[i] = pass_log_c(s.len[i]);
         if (s.npass > 1 && s.len[i] < 5) {
@@ -307,7 +319,7 @@ extern "C" onefft_plan *onefft_plan_create_bf16x3(size_t n, int require_accepted
 }
 
 extern "C" onefft_plan *onefft_plan_create_split(size_t n, int npass, const int *log2_len) {
-    return onefft_plan_create_tiles(n, npass, log2_len, nullptr, 1, 0);
+    return onefft_plan_create_tiles(n, npass, log2_len, nullptr, ONEFFT_OPT_L2_KEEP, 0);
 }
 
 extern "C" void onefft_plan_destroy(onefft_plan *plan) {
@@ -354,6 +366,15 @@ static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *
     a.lo_bits = p->lo_bits;
     a.l2_keep = p->l2_keep;
     a.tli = 31;
+    a.err = p->err;
+    // pass i through its TMA kernel where the plan asks for it and the shape and buffers allow
+    const bool use_tma = p->tma && !p->tc && batch <= 65535 && ((((uintptr_t)in | (uintptr_t)out) & 15) == 0);
+    auto run = [&](int mode, int i, const PassArgs &x) {
+        if (use_tma && pass_tma_supported(p->len[i], p->cols[i]))
+            return launch_pass_tma(mode, p->len[i], p->cols[i], x, (int)batch, s);
+        return p->tc ? launch_pass_tc(mode, p->len[i], x, (int)batch, s)
+                     : launch_pass(mode, p->len[i], p->cols[i], x, (int)batch, s);
+    };
     if (p->npass == 3 && p->chunk > 0) {
         // Passes 0 and 1 of a three-pass transform n = A B C run chunk by chunk over the last
         // digit j_c: pass 1 on columns j_c needs only pass 0's outputs for the same j_c, which
@@ -386,8 +407,8 @@ static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *
             c0.inner_base = g;
             c1.outer_base = g;
             g_launches.fetch_add(2);
-            cudaError_t e = launch_pass(0, A, p->cols[0], c0, (int)batch, s);
-            if (e == cudaSuccess) e = launch_pass(1, B, p->cols[1], c1, (int)batch, s);
+            cudaError_t e = run(0, 0, c0);
+            if (e == cudaSuccess) e = run(1, 1, c1);
             if (e != cudaSuccess) return e;
         }
         a.in = out;
@@ -397,7 +418,7 @@ static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *
         a.swap_out = inverse;
         a.log_s = A + B;
         g_launches.fetch_add(1);
-        return launch_pass(2, Cd, p->cols[2], a, (int)batch, s);
+        return run(2, 2, a);
     }
     int done = 0;  // log2 of the digits transformed so far
     for (int i = 0; i < p->npass; ++i) {
@@ -416,8 +437,7 @@ static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *
         }
         int mode = first ? 0 : last ? 2 : 1;
         g_launches.fetch_add(1);
-        cudaError_t e = p->tc ? launch_pass_tc(mode, p->len[i], a, (int)batch, s)
-                              : launch_pass(mode, p->len[i], p->cols[i], a, (int)batch, s);
+        cudaError_t e = run(mode, i, a);
         if (e != cudaSuccess) return e;
         done += p->len[i];
     }
@@ -586,6 +606,17 @@ struct DeviceGuard {
 
 }  // namespace
 
+// After a synchronise: 0, or an error if a TMA kernel of the plan recorded an expired wait in
+// the plan's error word (which is then cleared).
+static int kernel_error(const onefft_plan *p) {
+    if (!p->tma) return 0;
+    unsigned flag = 0;
+    if (cudaMemcpy(&flag, p->err, sizeof flag, cudaMemcpyDeviceToHost) != cudaSuccess) return cuda_error(cudaGetLastError(), "error word");
+    if (!flag) return 0;
+    cudaMemset(p->err, 0, sizeof flag);
+    return set_error(ONEFFT_ERR_CUDA_BASE, "a bulk tensor copy did not complete in time (code %u)", flag);
+}
+
 // One transform (or `batch`) through host or device buffers, synchronous. Returns 0 or an error;
 // `out` is written only by the final copy, after every kernel succeeded.
 static int host_execute(const onefft_plan *p, const float *in, float *out, size_t batch, int inverse) {
@@ -604,7 +635,8 @@ static int host_execute(const onefft_plan *p, const float *in, float *out, size_
         // device memory of the caller: transform in place of the caller's buffers
         e = plan_enqueue(p, (const float2 *)in, (float2 *)out, (long long)batch, inverse, ctx->stream[0]);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream[0]);
-        return e == cudaSuccess ? 0 : cuda_error(e, "transform");
+        if (e != cudaSuccess) return cuda_error(e, "transform");
+        return kernel_error(p);
     }
     // Chunks of whole transforms, round-robin over the streams: chunk k's copy-in overlaps the
     // kernels and copy-out of chunks k-1 and k-2.
@@ -639,6 +671,7 @@ static int host_execute(const onefft_plan *p, const float *in, float *out, size_
             // single chunk: check the kernels before the output is touched
             e = cudaStreamSynchronize(s);
             if (e != cudaSuccess) break;
+            if (kernel_error(p)) return ONEFFT_ERR_CUDA_BASE;
         }
         e = cudaMemcpyAsync((char *)out + first * tbytes, d_out, cnt * tbytes, cudaMemcpyDefault, s);
         if (e != cudaSuccess) break;
@@ -649,7 +682,8 @@ static int host_execute(const onefft_plan *p, const float *in, float *out, size_
         if (e2 == cudaSuccess) e2 = es;
     }
     if (e == cudaSuccess) e = e2;
-    return e == cudaSuccess ? 0 : cuda_error(e, "transform");
+    if (e != cudaSuccess) return cuda_error(e, "transform");
+    return kernel_error(p);
 }
 
 extern "C" void onefft_plan_forward(const onefft_plan *plan, const float *in, float *out) {

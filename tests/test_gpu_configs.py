@@ -120,7 +120,7 @@ def test_config2_single_2p27(ofb, oracle):
     n = 1 << log2n
     x = oracle.gen_normal(2 * n, 0x27)
     plan = ofb.Plan(n)
-    assert plan.passes() == (9, 9, 9)
+    assert len(plan.passes()) == 3 and sum(plan.passes()) == 27
     d_in = T.from_numpy(x).cuda()
     d_out = T.empty_like(d_in)
     d_back = T.empty_like(d_in)

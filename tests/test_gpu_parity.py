@@ -207,13 +207,39 @@ SHAPES = [  # (n, split, tile widths, chunk)
 ]
 
 
-@pytest.mark.parametrize("n,split,cols,chunk", [(n, s, None, 0) for n, s in SPLITS] + SHAPES)
-def test_pass_splits(ofb, oracle, n, split, cols, chunk):
-    """Every pass kernel (all tile lengths 2^4..2^12, widths 4..16, first/middle/last, chunked
-    first passes) against FP64."""
+TMA_SHAPES = [  # (n, split, tile widths, chunk) run through the bulk-tensor-copy kernels
+    (1 << 12, (6, 6), (4, 4), 0), (1 << 16, (8, 8), (2, 3), 0), (1 << 18, (9, 9), (4, 3), 0),
+    (1 << 20, (10, 10), (1, 2), 0), (1 << 22, (11, 11), (2, 1), 0), (1 << 24, (12, 12), (1, 1), 0),
+    (1 << 21, (7, 7, 7), (4, 3, 4), 5), (1 << 24, (8, 8, 8), (4, 4, 4), 0), (1 << 23, (9, 7, 7), (3, 4, 3), 0),
+]
+
+
+@pytest.mark.parametrize("n,split,cols,chunk,tma", [(n, s, None, 0, False) for n, s in SPLITS] +
+                         [s + (False,) for s in SHAPES] + [s + (True,) for s in TMA_SHAPES])
+def test_pass_splits(ofb, oracle, n, split, cols, chunk, tma):
+    """Every pass kernel (all tile lengths 2^4..2^12, widths 2..16, first/middle/last, chunked
+    first passes, plain and TMA-staged) against FP64; TMA results equal the plain kernels'."""
     log2n = n.bit_length() - 1
     x = oracle.gen_normal(2 * n, 1000 + log2n)
-    plan = ofb.Plan(n, split=split, cols=cols, chunk=chunk)
+    plan = ofb.Plan(n, split=split, cols=cols, chunk=chunk, tma=tma)
+    if tma:
+        import torch
+        plain = ofb.Plan(n, split=split, cols=cols, chunk=chunk)
+        d = torch.from_numpy(x).cuda()
+        a, b = torch.empty_like(d), torch.empty_like(d)
+        for inv in (False, True):
+            (plan.dev_inverse if inv else plan.dev_forward)(d.data_ptr(), a.data_ptr(), 1)
+            (plain.dev_inverse if inv else plain.dev_forward)(d.data_ptr(), b.data_ptr(), 1)
+            torch.cuda.synchronize()
+            assert torch.equal(a, b), (n, split, inv)
+        # batched through the TMA kernels too (the batch is the copies' outermost dimension)
+        xb = torch.from_numpy(oracle.gen_normal(6 * n, 77)).cuda()
+        ya, yb = torch.empty_like(xb), torch.empty_like(xb)
+        plan.dev_forward(xb.data_ptr(), ya.data_ptr(), 3)
+        plain.dev_forward(xb.data_ptr(), yb.data_ptr(), 3)
+        torch.cuda.synchronize()
+        assert torch.equal(ya, yb)
+        plain.destroy()
     assert plan.passes() == split
     default = ofb.Plan(n)
     for inv in (False, True):
