@@ -29,7 +29,7 @@ struct PassArgs {
     unsigned outer_base;
     unsigned inner_base;
     unsigned ntiles;  // grid size of the launch (tiles per transform)
-    unsigned* err;    // plan's error word: set by a kernel whose bounded wait ran out
+    unsigned* err;    // plan's error word (mapped host memory): set by a kernel whose bounded wait ran out
 };
 
 // Largest size handled by one kernel (k_tiny / k_batched).

@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4))
                                             ((t & ((1u << a.tli) - 1)) << LOG_C);
     const int q0 = (int)(col0 & ((1u << a.log_s) - 1)), h = (int)(col0 >> a.log_s);
     if (smem_u32(smem) & 127) {  // bulk tensor copies need a 128-byte aligned destination
-        if (tid == 0) atomicExch(a.err, 2u);
+        if (tid == 0) *(volatile unsigned*)a.err = 2u;
         return;
     }
     if (tid == 0) {
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4))
     const bool ok = mbar_wait(bar, 0);
     if (__syncthreads_or(!ok)) {
         if (tid == 0) {
-            atomicExch(a.err, 1u);
+            *(volatile unsigned*)a.err = 1u;
             mbar_wait(bar, 0);  // let a late copy land before the block's memory is released
         }
         return;

@@ -94,7 +94,8 @@ struct onefft_plan {
     int chunk;             // three passes: log2 of the last-digit columns per chunk of passes 0+1 (0 = none)
     int tc;                // radix-16 stages as split-BF16 tensor-core products (onefft_plan_create_bf16x3)
     int tma;               // passes staged through bulk tensor copies where the tile shape has a TMA kernel
-    unsigned *err;         // device word: set by a kernel whose bounded wait ran out
+    unsigned *err;         // error word as kernels address it: set by a kernel whose bounded wait ran out
+    unsigned *err_host;    // the same word on the host (mapped pinned memory: read without a copy)
     void *mem;             // the one device allocation
     size_t mem_bytes;
     const float2 *stw[3];  // stage twiddles of each pass's length
@@ -213,8 +214,6 @@ static onefft_plan *plan_build(size_t n, int m, const Shape &shape) {
         hi_off = bytes;
         bytes = align256(bytes + sizeof(double2) * ((size_t)1 << (m - p->lo_bits)));
     }
-    const size_t err_off = bytes;  // the error word
-    bytes += 256;
     e = dev_alloc(&p->mem, bytes);
     if (e != cudaSuccess) {
         delete p;
@@ -224,10 +223,19 @@ static onefft_plan *plan_build(size_t n, int m, const Shape &shape) {
     }
     p->mem_bytes = bytes;
     char *base = (char *)p->mem;
-    p->err = (unsigned *)(base + err_off);
-    cudaStream_t s;
-    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMemsetAsync(p->err, 0, sizeof(unsigned), s);
+    // The error word lives in mapped pinned host memory: kernels write it over the bus (only
+    // when a wait expires) and a host call reads it with a plain load after its stream
+    // synchronises, so checking it needs no copy that could queue behind other threads' large
+    // transfers on a copy engine.
+    e = cudaHostAlloc((void **)&p->err_host, sizeof(unsigned), cudaHostAllocMapped | cudaHostAllocPortable);
+    if (e == cudaSuccess) {
+        *(volatile unsigned *)p->err_host = 0;
+        e = cudaHostGetDevicePointer((void **)&p->err, p->err_host, 0);
+    } else {
+        p->err_host = nullptr;
+    }
+    cudaStream_t s = nullptr;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
     if (e == cudaSuccess) {
         for (int i = 0; i < p->npass && e == cudaSuccess; ++i) {
             p->stw[i] = (const float2 *)(base + off[i]);
@@ -244,6 +252,7 @@ static onefft_plan *plan_build(size_t n, int m, const Shape &shape) {
     }
     if (e != cudaSuccess) {
         cudaFree(p->mem);
+        if (p->err_host) cudaFreeHost(p->err_host);
         delete p;
         cuda_error(e, "plan table build");
         return nullptr;
@@ -328,6 +337,7 @@ extern "C" void onefft_plan_destroy(onefft_plan *plan) {
     cudaGetDevice(&cur);
     if (cur != plan->device) cudaSetDevice(plan->device);
     cudaFree(plan->mem);
+    if (plan->err_host) cudaFreeHost(plan->err_host);
     if (cur >= 0 && cur != plan->device) cudaSetDevice(cur);
     delete plan;
 }
@@ -610,10 +620,10 @@ struct DeviceGuard {
 // the plan's error word (which is then cleared).
 static int kernel_error(const onefft_plan *p) {
     if (!p->tma) return 0;
-    unsigned flag = 0;
-    if (cudaMemcpy(&flag, p->err, sizeof flag, cudaMemcpyDeviceToHost) != cudaSuccess) return cuda_error(cudaGetLastError(), "error word");
+    volatile unsigned *word = p->err_host;
+    const unsigned flag = *word;
     if (!flag) return 0;
-    cudaMemset(p->err, 0, sizeof flag);
+    *word = 0;
     return set_error(ONEFFT_ERR_CUDA_BASE, "a bulk tensor copy did not complete in time (code %u)", flag);
 }
 
