@@ -77,11 +77,21 @@ __device__ __forceinline__ void tma_store_5d(const CUtensorMap* map, const void*
     asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
+// Blocks per SM that the register allocation must allow (0: the compiler chooses freely). Measured
+// on a B200: the last pass with 1024-value tiles of 8 columns (512 threads, 70 KB of shared
+// memory) fits 3 blocks per SM at 40 registers instead of 2 at 41, which hides more of the tile
+// copy's latency (2^27: 1.18 -> 1.12 ms). Caps on the other shapes were slower (spills, or more
+// blocks than the copy bandwidth needs).
+template <int LOG_L, int LOG_C, int MODE>
+constexpr int tma_min_blocks() {
+    return LOG_L == 10 && LOG_C == 3 && MODE == 2 ? 3 : 0;
+}
+
 // One tile per block; MODE as k_pass. `tin` maps the pass's input, `tout` its output (MODE 1/2:
 // the same array, in place). Shared memory: the tile (dense as the copy lands, then reused
 // padded by the exchanges), the inter-pass twiddle factors, the mbarrier.
 template <int LOG_L, int LOG_C, int MODE>
-__global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4))
+__global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_L, LOG_C, MODE>()))
     k_pass_tma(PassArgs a, const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout) {
     constexpr int L = 1 << LOG_L, T = L / 16, C = 1 << LOG_C;
     constexpr int ELO = L < 256 ? L : 256;

@@ -1,6 +1,7 @@
 """Runs one transform shape a few times, for an external profiler (ncu) to capture.
 
     python -m onefft_b200.profile_case --log2n 24 [--split 8,8,8 --cols 4,4,4] [--batch 1] [--reps 3]
+    python -m onefft_b200.profile_case --log2n 25 --split 8,7,10 --cols 4,4,3 --tma
     python -m onefft_b200.profile_case --log2n 12 --batch 4096            # the batched kernel
     python -m onefft_b200.profile_case --uneven 2000                      # the uneven-batch kernel
 
@@ -26,6 +27,7 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--inverse", action="store_true")
     ap.add_argument("--chunk", type=int, default=0, help="three passes: log2 last-digit columns per chunk")
+    ap.add_argument("--tma", action="store_true", help="with --split: TMA-staged passes")
     ap.add_argument("--uneven", type=int, default=0, help="run an uneven batch of this many transforms")
     args = ap.parse_args()
     g = torch.Generator(device="cuda").manual_seed(7)
@@ -45,7 +47,7 @@ def main():
     n = 1 << args.log2n
     split = tuple(int(v) for v in args.split.split(",")) if args.split else None
     cols = tuple(int(v) for v in args.cols.split(",")) if args.cols else None
-    plan = ofb.Plan(n, split=split, cols=cols, chunk=args.chunk)
+    plan = ofb.Plan(n, split=split, cols=cols, chunk=args.chunk, tma=args.tma)
     x = torch.randn(2 * n * args.batch, device="cuda", generator=g)
     y = torch.empty_like(x)
     f = plan.dev_inverse if args.inverse else plan.dev_forward
