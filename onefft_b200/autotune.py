@@ -79,6 +79,7 @@ def main():
     ap.add_argument("--reps", type=int, default=7)
     ap.add_argument("--out", default=None)
     ap.add_argument("--max-candidates", type=int, default=1000)
+    ap.add_argument("--tma-only", action="store_true", help="only TMA-staged variants, no chunked passes")
     args = ap.parse_args()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     results = {}
@@ -96,6 +97,8 @@ def main():
         cands = candidates(m)[: args.max_candidates]
         variants = [(ls, cs, g, keep, tma) for ls, cs, g in cands for keep in (True, False)
                     for tma in ((False, True) if any(tma_ok(l, c) for l, c in zip(ls, cs)) else (False,))]
+        if args.tma_only:
+            variants = [v for v in variants if v[4] and not v[2]]
         for ls, cs, g, keep, tma in variants:
             if True:
                 try:
