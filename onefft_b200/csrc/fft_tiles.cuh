@@ -19,6 +19,43 @@ __device__ __forceinline__ double2 big_twiddle_f64(const double2* __restrict__ l
     return zmul(__ldg(lo + (t & ((1u << lo_bits) - 1))), __ldg(hi + (t >> lo_bits)));
 }
 
+// w^e for e < 2^BITS by square-and-multiply in FP64. With w from the two-level tables (error
+// ~1e-16), the result is within ~BITS * 2^(BITS+1) * 1e-16 of exact, far below FP32 rounding.
+template <int BITS>
+__device__ __forceinline__ double2 zpow(double2 w, unsigned e) {
+    double2 r = make_double2(1.0, 0.0);
+#pragma unroll
+    for (int b = 0; b < BITS; ++b) {
+        if ((e >> b) & 1u) r = zmul(r, w);
+        if (b + 1 < BITS) w = zmul(w, w);
+    }
+    return r;
+}
+
+// Inter-pass twiddles of a pass tile: output j + T kk of a column with factor F (first pass:
+// the column index; middle pass: S h) is multiplied by w_n^(F j) * w_n^(F T kk), each factor
+// rounded once to FP32. Both factors are powers of ONE table product per column (w_n^F and
+// w_n^(F T)), so a tile reads the FP64 tables at C addresses instead of once per factor.
+// The 16 factors w_n^(F T kk) of each column go to shared memory (rows of 17).
+template <int LOG_L, int LOG_C, int MODE>
+__device__ __forceinline__ void pass_twiddle_rows(const PassArgs& a, unsigned col0, float2* tws, int tid, int nthreads) {
+    constexpr unsigned T = 1u << (LOG_L - 4);
+    constexpr int C = 1 << LOG_C;
+    const unsigned hs = (col0 >> a.log_s) << a.log_s;
+    for (int i = tid; i < (MODE == 0 ? C : 1) * 16; i += nthreads) {
+        const int cc = i >> 4, kk = i & 15;
+        const unsigned f = MODE == 0 ? col0 + cc : hs;
+        const double2 w = zpow<4>(big_twiddle_f64(a.tw_lo, a.tw_hi, a.lo_bits, f * T), (unsigned)kk);
+        tws[cc * 17 + kk] = make_float2((float)w.x, (float)w.y);
+    }
+}
+// ... and the thread's own factor w_n^(F j).
+template <int LOG_L>
+__device__ __forceinline__ float2 pass_twiddle_lane(const PassArgs& a, unsigned f, int j) {
+    const double2 w = zpow<LOG_L - 4>(big_twiddle_f64(a.tw_lo, a.tw_hi, a.lo_bits, f), (unsigned)j);
+    return make_float2((float)w.x, (float)w.y);
+}
+
 // Loads of data the kernel never writes go through the read-only path; the intermediate array
 // between passes may be kept in L2 for the next pass (evict last).
 __device__ __forceinline__ float2 ld_stream(const float2* p) { return __ldg(p); }
@@ -109,19 +146,15 @@ __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long lo
         base = q + (h << (a.log_s + LOG_L));
     }
     // Inter-pass twiddles w_n^(F (j + T kk)) for this thread's outputs, F = r (first pass,
-    // per column) or S h (middle pass, per tile), split as w^(F j) * w^(F T kk): the 16 factors
-    // w^(F T kk) of each column are evaluated once per tile from the FP64 tables into shared
-    // memory (rows padded to 17 so the columns of a warp hit distinct banks), w^(F j) once per
-    // thread; each is rounded once to FP32 and their product applied in FP32.
+    // per column) or S h (middle pass, per tile), split as w^(F j) * w^(F T kk): the factors
+    // w^(F T kk) of each column in shared memory (rows padded to 17 so the columns of a warp hit
+    // distinct banks), w^(F j) per thread; each rounded once to FP32, their product applied in
+    // FP32 (pass_twiddle_rows / pass_twiddle_lane).
     float2* tws = smem + spad(C * L - 1) + 1;
+    float2 wjf = make_float2(1.f, 0.f);
     if (MODE != 2) {
-        const unsigned hs = (col0 >> a.log_s) << a.log_s;
-        for (int i = tid; i < (MODE == 0 ? C : 1) * 16; i += C * T) {
-            const int cc = i >> 4, kk = i & 15;
-            const unsigned f = MODE == 0 ? col0 + cc : hs;
-            double2 w = big_twiddle_f64(a.tw_lo, a.tw_hi, a.lo_bits, f * (unsigned)T * (unsigned)kk);
-            tws[cc * 17 + kk] = make_float2((float)w.x, (float)w.y);
-        }
+        pass_twiddle_rows<LOG_L, LOG_C, MODE>(a, col0, tws, tid, C * T);
+        wjf = pass_twiddle_lane<LOG_L>(a, MODE == 0 ? col0 + c : (col0 >> a.log_s) << a.log_s, j);
     }
     // element j + T k of the column: p0 + k * estep
     const long long estep = (long long)T << a.log_s;
@@ -141,9 +174,6 @@ __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long lo
     else tile_fft<LOG_L, C>(v, j, a.stw, smem, c);
     if (MODE != 2) {
         if (Stages<LOG_L>::COUNT == 1) __syncthreads();  // tile_fft had no barrier to publish tws
-        const unsigned f = MODE == 0 ? col0 + c : (col0 >> a.log_s) << a.log_s;
-        const double2 wj = big_twiddle_f64(a.tw_lo, a.tw_hi, a.lo_bits, f * (unsigned)j);
-        const float2 wjf = make_float2((float)wj.x, (float)wj.y);
         const float2* tw = tws + (MODE == 0 ? c * 17 : 0);
 #pragma unroll
         for (int k = 0; k < 16; ++k) v[k] = cmul(v[k], cmul(wjf, tw[k]));

@@ -119,14 +119,10 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_
     (void)ELO;
     // inter-pass twiddle factors (as pass_tile) while the copy is in flight
     float2* tws = smem + spad(C * L - 1) + 1;
+    float2 wjf = make_float2(1.f, 0.f);
     if (MODE != 2) {
-        const unsigned hs = (col0 >> a.log_s) << a.log_s;
-        for (int i = tid; i < (MODE == 0 ? C : 1) * 16; i += C * T) {
-            const int cc = i >> 4, kk = i & 15;
-            const unsigned f = MODE == 0 ? col0 + cc : hs;
-            double2 w = big_twiddle_f64(a.tw_lo, a.tw_hi, a.lo_bits, f * (unsigned)T * (unsigned)kk);
-            tws[cc * 17 + kk] = make_float2((float)w.x, (float)w.y);
-        }
+        pass_twiddle_rows<LOG_L, LOG_C, MODE>(a, col0, tws, tid, C * T);
+        wjf = pass_twiddle_lane<LOG_L>(a, MODE == 0 ? col0 + c : (col0 >> a.log_s) << a.log_s, j);
     }
     __syncthreads();  // the barrier is initialised before anyone waits on it
     const bool ok = mbar_wait(bar, 0);
@@ -147,9 +143,6 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_
     tile_fft<LOG_L, C>(v, j, a.stw, smem, c);
     if (MODE != 2) {
         if (Stages<LOG_L>::COUNT == 1) __syncthreads();
-        const unsigned f = MODE == 0 ? col0 + c : (col0 >> a.log_s) << a.log_s;
-        const double2 wj = big_twiddle_f64(a.tw_lo, a.tw_hi, a.lo_bits, f * (unsigned)j);
-        const float2 wjf = make_float2((float)wj.x, (float)wj.y);
         const float2* tw = tws + (MODE == 0 ? c * 17 : 0);
 #pragma unroll
         for (int k = 0; k < 16; ++k) v[k] = cmul(v[k], cmul(wjf, tw[k]));
