@@ -122,6 +122,34 @@ def test_uneven_all_sizes_and_gaps(ofb, oracle):
     batch.destroy()
 
 
+def test_uneven_in_block_passes_repeatable(ofb, oracle):
+    """Many 2^13 .. 2^16 transforms, each run by one block as two passes of tile after tile, at
+    8-byte (not 16-byte) aligned offsets: ten executions equal the first bit for bit and the
+    2^15 / 2^16 results equal the plain path's. A block that reused a tile's shared memory
+    before its slowest warp had read it would show up as a run that differs."""
+    T = torch()
+    rng = np.random.default_rng(23)
+    log2n = rng.integers(13, 17, 600).astype(np.int32)
+    inverse = (rng.random(log2n.size) < 0.5).astype(np.int32)
+    sizes = (1 << log2n.astype(np.int64)) + 1
+    offset = np.concatenate([[1], 1 + np.cumsum(sizes)[:-1]]).astype(np.int64)
+    span = int(offset[-1] + (1 << int(log2n[-1])))
+    x, _ = oracle.gen_uniform(2 * span, 23)
+    batch = ofb.UnevenBatch(log2n, inverse, offset)
+    d_in = T.from_numpy(x).cuda()
+    first = T.zeros_like(d_in)
+    batch.execute(d_in.data_ptr(), first.data_ptr())
+    again = T.zeros_like(d_in)
+    for _ in range(10):
+        batch.execute(d_in.data_ptr(), again.data_ptr())
+        T.cuda.synchronize()
+        assert T.equal(again, first)
+    big = log2n >= 15
+    want = plain_path(ofb, T, log2n[big], inverse[big], offset[big], d_in)
+    compare(oracle, log2n[big], offset[big], first, want)
+    batch.destroy()
+
+
 def test_uneven_rejects_bad_arguments(ofb):
     T = torch()
     L = ofb.lib()
