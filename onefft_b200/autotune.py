@@ -80,6 +80,7 @@ def main():
     ap.add_argument("--out", default=None)
     ap.add_argument("--max-candidates", type=int, default=1000)
     ap.add_argument("--tma-only", action="store_true", help="only TMA-staged variants, no chunked passes")
+    ap.add_argument("--chunked-only", action="store_true", help="only TMA-staged variants with L2-resident chunks")
     args = ap.parse_args()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     results = {}
@@ -99,6 +100,8 @@ def main():
                     for tma in ((False, True) if any(tma_ok(l, c) for l, c in zip(ls, cs)) else (False,))]
         if args.tma_only:
             variants = [v for v in variants if v[4] and not v[2]]
+        if args.chunked_only:
+            variants = [v for v in variants if v[4] and v[2]]
         for ls, cs, g, keep, tma in variants:
             if True:
                 try:

@@ -353,6 +353,6 @@ def test_allocation_failure_leaves_output_untouched(ofb):
 
 
 def test_max_abs_report(ofb):
-    """Prints the per-size max-abs errors gathered by test_size (north_star asks them stated)."""
+    """Prints the per-size max-abs errors gathered by test_size (the parity rule states them per size)."""
     for (l, d), v in sorted(MAX_ABS.items()):
         print(f"n=2^{l} {d}: max-abs {v:.3g}")

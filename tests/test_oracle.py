@@ -1,4 +1,4 @@
-"""CPU tests of the oracle: it must reproduce the reference before it may judge the GPU path.
+"""CPU tests of the oracle: it must reproduce the reference before it may check the GPU path.
 
 Pins (reference file:line in OneFFT):
   * the restated portable transform equals the reference's own ONEFFT_NO_SIMD build bit for bit
