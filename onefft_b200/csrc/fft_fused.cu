@@ -12,8 +12,13 @@
 
 namespace ofb {
 
+// Tiles of 2^11 .. 2^14 values are sized for 64 registers per thread (4 blocks of 256 threads or
+// 2 of 512 per SM, without spills): left to itself the compiler took up to 80, which held the
+// 8192-point tile to ONE block per SM (ncu: 24 % DRAM throughput, latency-bound); measured on a
+// B200, 4096 x 8192 went from 256 to 220 us and 512 x 8192 from 43.7 to 41.2 us. Smaller tiles
+// keep the compiler's choice (at 64 registers some spill and run slower).
 template <int LOG_L, int LOG_C>
-__global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4))
+__global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), LOG_L >= 11 ? 65536 / (64 << (LOG_L + LOG_C - 4)) : 0)
     k_power_loss_grad(const float2* __restrict__ x, const float* __restrict__ w, float2* __restrict__ grad,
                       double* __restrict__ loss, long long batch, const float2* __restrict__ stw) {
     constexpr int L = 1 << LOG_L, T = L / 16, THREADS = 1 << (LOG_L + LOG_C - 4);

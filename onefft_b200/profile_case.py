@@ -4,6 +4,8 @@
     python -m onefft_b200.profile_case --log2n 25 --split 8,7,10 --cols 4,4,3 --tma
     python -m onefft_b200.profile_case --log2n 12 --batch 4096            # the batched kernel
     python -m onefft_b200.profile_case --uneven 2000                      # the uneven-batch kernel
+    python -m onefft_b200.profile_case --log2n 13 --batch 512 --loss      # fused loss + gradient
+    python -m onefft_b200.profile_case --log2n 16 --batch 256 --bf16x3    # split-BF16 tensor cores
 
 Inputs are seeded standard-normal values on the device; the plan (and its table kernels) is
 built before the timed transforms, so `ncu -k regex:k_pass -s <n>` can skip to them.
@@ -28,6 +30,8 @@ def main():
     ap.add_argument("--inverse", action="store_true")
     ap.add_argument("--chunk", type=int, default=0, help="three passes: log2 last-digit columns per chunk")
     ap.add_argument("--tma", action="store_true", help="with --split: TMA-staged passes")
+    ap.add_argument("--loss", action="store_true", help="the fused weighted-power loss and gradient")
+    ap.add_argument("--bf16x3", action="store_true", help="the split-BF16 tensor-core plan")
     ap.add_argument("--uneven", type=int, default=0, help="run an uneven batch of this many transforms")
     args = ap.parse_args()
     g = torch.Generator(device="cuda").manual_seed(7)
@@ -47,7 +51,20 @@ def main():
     n = 1 << args.log2n
     split = tuple(int(v) for v in args.split.split(",")) if args.split else None
     cols = tuple(int(v) for v in args.cols.split(",")) if args.cols else None
-    plan = ofb.Plan(n, split=split, cols=cols, chunk=args.chunk, tma=args.tma)
+    plan = ofb.Plan(n, bf16x3=True) if args.bf16x3 else ofb.Plan(n, split=split, cols=cols, chunk=args.chunk, tma=args.tma)
+    if args.loss:
+        x = torch.randn(2 * n * args.batch, device="cuda", generator=g)
+        w = torch.rand(n, device="cuda", generator=g)
+        grad = torch.empty_like(x)
+        loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+        for _ in range(args.reps):
+            rc = ofb.lib().onefft_dev_weighted_power_loss(plan.handle, x.data_ptr(), w.data_ptr(), grad.data_ptr(),
+                                                          args.batch, loss.data_ptr(), None)
+            if rc:
+                raise RuntimeError(ofb.last_error())
+        torch.cuda.synchronize()
+        print(f"fused loss n=2^{args.log2n} x {args.batch}: {args.reps} runs, loss {loss.item():.6g}")
+        return
     x = torch.randn(2 * n * args.batch, device="cuda", generator=g)
     y = torch.empty_like(x)
     f = plan.dev_inverse if args.inverse else plan.dev_forward
