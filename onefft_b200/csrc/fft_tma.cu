@@ -77,6 +77,42 @@ __device__ __forceinline__ void tma_store_5d(const CUtensorMap* map, const void*
     asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
+// The same copies with an L2 eviction-priority hint (a createpolicy value).
+__device__ __forceinline__ void tma_load_4d_hint(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                                 uint64_t* bar, unsigned long long policy) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, "
+        "{%2, %3, %4, %5}], [%6], %7;" ::"r"(smem_u32(dst)),
+        "l"((unsigned long long)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_5d_hint(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                                 int c4, uint64_t* bar, unsigned long long policy) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, "
+        "{%2, %3, %4, %5, %6}], [%7], %8;" ::"r"(smem_u32(dst)),
+        "l"((unsigned long long)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_store_5d_hint(const CUtensorMap* map, const void* src, int c0, int c1, int c2,
+                                                  int c3, int c4, unsigned long long policy) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.global.shared::cta.tile.bulk_group.L2::cache_hint [%0, {%2, %3, %4, %5, %6}], [%1], "
+        "%7;" ::"l"((unsigned long long)map),
+        "r"(smem_u32(src)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "l"(policy)
+        : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+__device__ __forceinline__ unsigned long long policy_evict_first() {
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
 // Blocks per SM that the register allocation must allow (0: the compiler chooses freely). Measured
 // on a B200: the last pass with 1024-value tiles of 8 columns (512 threads, 70 KB of shared
 // memory) fits 3 blocks per SM at 40 registers instead of 2 at 41, which hides more of the tile
@@ -113,8 +149,17 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_
     if (tid == 0) {
         mbar_init(bar, 1);
         mbar_expect_tx(bar, (unsigned)(C * L * sizeof(float2)));
-        if (MODE == 0) tma_load_4d(smem, &tin, (int)col0, 0, 0, b, bar);
-        else tma_load_5d(smem, &tin, q0, 0, 0, h, b, bar);
+        // With l2_keep the array between passes should stay in L2: the input (read once) and
+        // the last pass's tile (read for the last time) are loaded evict-first.
+        if (a.l2_keep && MODE != 1) {
+            const unsigned long long first = policy_evict_first();
+            if (MODE == 0) tma_load_4d_hint(smem, &tin, (int)col0, 0, 0, b, bar, first);
+            else tma_load_5d_hint(smem, &tin, q0, 0, 0, h, b, bar, first);
+        } else if (MODE == 0) {
+            tma_load_4d(smem, &tin, (int)col0, 0, 0, b, bar);
+        } else {
+            tma_load_5d(smem, &tin, q0, 0, 0, h, b, bar);
+        }
     }
     (void)ELO;
     // inter-pass twiddle factors (as pass_tile) while the copy is in flight
@@ -161,14 +206,24 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_
         float2* q = a.out + ((long long)b << a.log2n) + (((j1 + (j2 << a.rev_b1)) << LOG_L) + kk0);
         const float2* r = smem + spad(kk0 * C + cc);
 #pragma unroll
-        for (int i = 0; i < 16; ++i) q[i * T] = r[padc(i * T * C)];
+        if (a.l2_keep) {
+            const unsigned long long keep = policy_evict_last();  // the next pass reads these
+#pragma unroll
+            for (int i = 0; i < 16; ++i) st_policy(q + i * T, r[padc(i * T * C)], keep);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) q[i * T] = r[padc(i * T * C)];
+        }
     } else {
         // dense tile back in shared memory, then one bulk tensor store
 #pragma unroll
         for (int k = 0; k < 16; ++k) smem[(j + T * k) * C + c] = a.swap_out ? swap_ri(v[k]) : v[k];
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
-        if (tid == 0) tma_store_5d(&tout, smem, q0, 0, 0, h, b);
+        if (tid == 0) {
+            if (MODE == 1 && a.l2_keep) tma_store_5d_hint(&tout, smem, q0, 0, 0, h, b, policy_evict_last());
+            else tma_store_5d(&tout, smem, q0, 0, 0, h, b);
+        }
     }
 }
 

@@ -121,19 +121,19 @@ struct Shape {
 // 2^16 keeps the (8, 8) split (as fast as the best) so the uneven batch's in-block passes,
 // which use it, stay bit-identical to this path.
 static const Shape kTuned[] = {
-    /* 15 */ {2, {8, 7, 0}, {3, 4, 0}, 1, 0, 1},
-    /* 16 */ {2, {8, 8, 0}, {3, 3, 0}, 1, 0, 1},
+    /* 15 */ {2, {8, 7, 0}, {3, 4, 0}, 0, 0, 1},
+    /* 16 */ {2, {8, 8, 0}, {3, 3, 0}, 0, 0, 1},
     /* 17 */ {2, {10, 7, 0}, {1, 4, 0}, 0, 0, 0},
     /* 18 */ {2, {10, 8, 0}, {2, 3, 0}, 0, 0, 0},
     /* 19 */ {2, {8, 11, 0}, {4, 1, 0}, 1, 0, 0},
-    /* 20 */ {2, {11, 9, 0}, {1, 4, 0}, 1, 0, 1},
-    /* 21 */ {2, {11, 10, 0}, {2, 3, 0}, 1, 0, 0},
+    /* 20 */ {2, {12, 8, 0}, {1, 3, 0}, 1, 0, 1},
+    /* 21 */ {2, {11, 10, 0}, {1, 4, 0}, 0, 0, 1},
     /* 22 */ {3, {8, 7, 7}, {3, 4, 4}, 1, 0, 1},
     /* 23 */ {3, {8, 8, 7}, {3, 4, 4}, 1, 0, 1},
     /* 24 */ {3, {8, 8, 8}, {3, 3, 3}, 0, 0, 1},
-    /* 25 */ {3, {8, 8, 9}, {3, 3, 3}, 1, 0, 1},
-    /* 26 */ {3, {8, 9, 9}, {3, 3, 3}, 1, 0, 1},
-    /* 27 */ {3, {8, 9, 10}, {4, 3, 3}, 1, 0, 1},
+    /* 25 */ {3, {8, 8, 9}, {3, 3, 3}, 0, 0, 1},
+    /* 26 */ {3, {8, 8, 10}, {3, 3, 3}, 0, 0, 1},
+    /* 27 */ {3, {8, 9, 10}, {4, 3, 3}, 0, 0, 1},
 };
 
 static Shape tuned_shape(int m) {
