@@ -45,6 +45,20 @@ ONEFFT_API int onefft_dev_inverse_batched(const onefft_plan *plan, const float *
 ONEFFT_API int onefft_dev_adjoint_batched(const onefft_plan *plan, const float *d_grad_out, float *d_grad_in, size_t batch,
                                void *stream);
 
+/* Transforms with pointwise complex weights applied inside the kernels that read the input and
+ * write the output, so the weighting costs no extra pass over the data:
+ *   d_out_b = d_post * T(d_pre * d_in_b)      for each of the `batch` transforms b,
+ * T the plan's unnormalised forward (or inverse) transform, `*` elementwise complex products.
+ * d_pre and d_post are device arrays of n interleaved complex values shared by the whole batch
+ * (8-byte aligned, not overlapping d_out); either may be NULL (no weights on that side). Typical
+ * uses: windows and phase ramps before the transform, filters or normalisation after it. Same
+ * rules as onefft_dev_forward_batched otherwise; split-BF16 plans return ONEFFT_ERR_ARG. OneFFT
+ * has no counterpart (its callers multiply in separate loops). */
+ONEFFT_API int onefft_dev_forward_weighted(const onefft_plan *plan, const float *d_in, float *d_out, size_t batch,
+                                           const float *d_pre, const float *d_post, void *stream);
+ONEFFT_API int onefft_dev_inverse_weighted(const onefft_plan *plan, const float *d_in, float *d_out, size_t batch,
+                                           const float *d_pre, const float *d_post, void *stream);
+
 /* Loss and gradient of a weighted power spectrum in one pass over the data:
  *   *d_loss = sum over the batch and k of w[k]^2 |(F x_b)[k]|^2          (double, on the device)
  *   d_grad  = F^H (2 w^2 * F x_b) per transform (d loss / d conj(x), torch's convention; NULL =

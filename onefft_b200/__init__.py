@@ -30,6 +30,7 @@ C_SYMBOLS = (
     "onefft_plan_create", "onefft_plan_destroy", "onefft_plan_forward", "onefft_plan_inverse",
     "onefft_plan_size", "onefft_implementation",
     "onefft_dev_forward_batched", "onefft_dev_inverse_batched", "onefft_dev_adjoint_batched",
+    "onefft_dev_forward_weighted", "onefft_dev_inverse_weighted",
     "onefft_dev_weighted_power_loss",
     "onefft_plan_forward_batched", "onefft_plan_inverse_batched",
     "onefft_plan_create_split", "onefft_plan_create_tiles", "onefft_plan_create_bf16x3", "onefft_plan_passes",
@@ -82,6 +83,10 @@ def lib() -> ctypes.CDLL:
     for name in ("onefft_dev_forward_batched", "onefft_dev_inverse_batched", "onefft_dev_adjoint_batched"):
         f = getattr(L, name)
         f.argtypes = [_vp, _vp, _vp, _sz, _vp]
+        f.restype = ctypes.c_int
+    for name in ("onefft_dev_forward_weighted", "onefft_dev_inverse_weighted"):
+        f = getattr(L, name)
+        f.argtypes = [_vp, _vp, _vp, _sz, _vp, _vp, _vp]
         f.restype = ctypes.c_int
     L.onefft_dev_weighted_power_loss.argtypes = [_vp, _vp, _vp, _vp, _sz, _vp, _vp]
     L.onefft_dev_weighted_power_loss.restype = ctypes.c_int
@@ -260,6 +265,16 @@ class Plan:
         rc = lib().onefft_dev_inverse_batched(self.handle, d_in, d_out, batch, stream)
         if rc != 0:
             raise RuntimeError(f"onefft_dev_inverse_batched failed ({rc}): {last_error()}")
+
+    def dev_weighted(self, d_in: int, d_out: int, batch: int = 1, pre: int | None = None, post: int | None = None,
+                     inverse: bool = False, stream: int = 0) -> None:
+        """out_b = post * T(pre * in_b) with the weights applied inside the transform kernels
+        (onefft_dev_forward_weighted / _inverse_weighted); pre / post are device pointers to n
+        complex values or None."""
+        f = lib().onefft_dev_inverse_weighted if inverse else lib().onefft_dev_forward_weighted
+        rc = f(self.handle, d_in, d_out, batch, pre, post, stream)
+        if rc != 0:
+            raise RuntimeError(f"onefft_dev_{'inverse' if inverse else 'forward'}_weighted failed ({rc}): {last_error()}")
 
     def dev_adjoint(self, d_grad_out: int, d_grad_in: int, batch: int = 1, stream: int = 0) -> None:
         rc = lib().onefft_dev_adjoint_batched(self.handle, d_grad_out, d_grad_in, batch, stream)

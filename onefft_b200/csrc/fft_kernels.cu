@@ -64,28 +64,32 @@ __global__ void k_twiddle_probe(float2* __restrict__ dst, unsigned log2n, unsign
 
 // ---- kernels --------------------------------------------------------------------------------------
 
-template <int LOG_N>
+// W: the pointwise weights pre / post are applied (instantiated only for weighted calls).
+template <int LOG_N, bool W>
 __global__ void __launch_bounds__(256) k_tiny(const float2* __restrict__ in, float2* __restrict__ out,
-                                              long long batch, int inverse) {
+                                              long long batch, int inverse, const float2* __restrict__ pre,
+                                              const float2* __restrict__ post) {
     long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= batch) return;
-    tiny_transform<LOG_N>(in + (g << LOG_N), out + (g << LOG_N), inverse);
+    tiny_transform<LOG_N, W>(in + (g << LOG_N), out + (g << LOG_N), inverse, pre, post);
 }
 
-template <int LOG_L, int LOG_C>
+template <int LOG_L, int LOG_C, bool W>
 __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4))
     k_batched(const float2* __restrict__ in, float2* __restrict__ out, long long batch,
-              const float2* __restrict__ stw, int inverse) {
+              const float2* __restrict__ stw, int inverse, const float2* __restrict__ pre,
+              const float2* __restrict__ post) {
     extern __shared__ float2 smem[];
     const int tid = threadIdx.x;
     const long long g = ((long long)blockIdx.x << LOG_C) + (tid >> (LOG_L - 4));
-    batched_tile<LOG_L, LOG_C>(in + (g << LOG_L), out + (g << LOG_L), g < batch, inverse, stw, smem, tid);
+    batched_tile<LOG_L, LOG_C, false, W>(in + (g << LOG_L), out + (g << LOG_L), g < batch, inverse, stw, smem, tid,
+                                         pre, post);
 }
 
-template <int LOG_L, int LOG_C, int MODE>
+template <int LOG_L, int LOG_C, int MODE, bool W>
 __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4)) k_pass(PassArgs a) {
     extern __shared__ float2 smem[];
-    pass_tile<LOG_L, LOG_C, MODE>(a, blockIdx.x, (long long)blockIdx.y << a.log2n, smem, threadIdx.x);
+    pass_tile<LOG_L, LOG_C, MODE, false, W>(a, blockIdx.x, (long long)blockIdx.y << a.log2n, smem, threadIdx.x);
 }
 
 // ---- launchers -------------------------------------------------------------------------------------
@@ -98,20 +102,20 @@ static cudaError_t set_smem(K kernel, int bytes) {
 
 int batched_log_c(int log_l) { return log_l >= 12 ? 0 : 12 - log_l; }
 
-template <int LOG_L>
-static cudaError_t launch_batched_t(const float2* in, float2* out, long long batch, const float2* stw, int inverse,
-                                    cudaStream_t stream) {
+template <int LOG_L, bool W>
+static cudaError_t launch_batched_w(const float2* in, float2* out, long long batch, const float2* stw, int inverse,
+                                    cudaStream_t stream, const float2* pre, const float2* post) {
     constexpr int LOG_C = LOG_L >= 12 ? 0 : 12 - LOG_L;
     constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
     constexpr int SMEM = smem_bytes(LOG_L, LOG_C);
-    auto kernel = k_batched<LOG_L, LOG_C>;
+    auto kernel = k_batched<LOG_L, LOG_C, W>;
     static cudaError_t attr = set_smem(kernel, SMEM);
     if (attr != cudaSuccess) return attr;
     const long long per_block = 1ll << LOG_C;
     long long blocks = (batch + per_block - 1) / per_block;
     while (blocks > 0) {  // gridDim.x limit 2^31-1
         long long now = blocks < 0x7fffffffll ? blocks : 0x7fffffffll;
-        kernel<<<(unsigned)now, THREADS, SMEM, stream>>>(in, out, batch, stw, inverse);
+        kernel<<<(unsigned)now, THREADS, SMEM, stream>>>(in, out, batch, stw, inverse, pre, post);
         long long done = now * per_block;
         in += done << LOG_L;
         out += done << LOG_L;
@@ -121,12 +125,22 @@ static cudaError_t launch_batched_t(const float2* in, float2* out, long long bat
     return cudaGetLastError();
 }
 
+template <int LOG_L>
+static cudaError_t launch_batched_t(const float2* in, float2* out, long long batch, const float2* stw, int inverse,
+                                    cudaStream_t stream, const float2* pre, const float2* post) {
+    return pre || post ? launch_batched_w<LOG_L, true>(in, out, batch, stw, inverse, stream, pre, post)
+                       : launch_batched_w<LOG_L, false>(in, out, batch, stw, inverse, stream, nullptr, nullptr);
+}
+
 template <int LOG_N>
-static cudaError_t launch_tiny_t(const float2* in, float2* out, long long batch, int inverse, cudaStream_t stream) {
+static cudaError_t launch_tiny_t(const float2* in, float2* out, long long batch, int inverse, cudaStream_t stream,
+                                 const float2* pre, const float2* post) {
+    const bool w = pre || post;
     long long blocks = (batch + 255) / 256;
     while (blocks > 0) {
         long long now = blocks < 0x7fffffffll ? blocks : 0x7fffffffll;
-        k_tiny<LOG_N><<<(unsigned)now, 256, 0, stream>>>(in, out, batch, inverse);
+        if (w) k_tiny<LOG_N, true><<<(unsigned)now, 256, 0, stream>>>(in, out, batch, inverse, pre, post);
+        else k_tiny<LOG_N, false><<<(unsigned)now, 256, 0, stream>>>(in, out, batch, inverse, nullptr, nullptr);
         long long done = now * 256;
         in += done << LOG_N;
         out += done << LOG_N;
@@ -137,24 +151,24 @@ static cudaError_t launch_tiny_t(const float2* in, float2* out, long long batch,
 }
 
 cudaError_t launch_single_kernel(int log2n, const float2* in, float2* out, long long batch, const float2* stw,
-                                 int inverse, cudaStream_t stream) {
+                                 int inverse, cudaStream_t stream, const float2* pre, const float2* post) {
     if (batch <= 0) return cudaSuccess;
     switch (log2n) {
-    case 0: return launch_tiny_t<0>(in, out, batch, inverse, stream);
-    case 1: return launch_tiny_t<1>(in, out, batch, inverse, stream);
-    case 2: return launch_tiny_t<2>(in, out, batch, inverse, stream);
-    case 3: return launch_tiny_t<3>(in, out, batch, inverse, stream);
-    case 4: return launch_batched_t<4>(in, out, batch, stw, inverse, stream);
-    case 5: return launch_batched_t<5>(in, out, batch, stw, inverse, stream);
-    case 6: return launch_batched_t<6>(in, out, batch, stw, inverse, stream);
-    case 7: return launch_batched_t<7>(in, out, batch, stw, inverse, stream);
-    case 8: return launch_batched_t<8>(in, out, batch, stw, inverse, stream);
-    case 9: return launch_batched_t<9>(in, out, batch, stw, inverse, stream);
-    case 10: return launch_batched_t<10>(in, out, batch, stw, inverse, stream);
-    case 11: return launch_batched_t<11>(in, out, batch, stw, inverse, stream);
-    case 12: return launch_batched_t<12>(in, out, batch, stw, inverse, stream);
-    case 13: return launch_batched_t<13>(in, out, batch, stw, inverse, stream);
-    case 14: return launch_batched_t<14>(in, out, batch, stw, inverse, stream);
+    case 0: return launch_tiny_t<0>(in, out, batch, inverse, stream, pre, post);
+    case 1: return launch_tiny_t<1>(in, out, batch, inverse, stream, pre, post);
+    case 2: return launch_tiny_t<2>(in, out, batch, inverse, stream, pre, post);
+    case 3: return launch_tiny_t<3>(in, out, batch, inverse, stream, pre, post);
+    case 4: return launch_batched_t<4>(in, out, batch, stw, inverse, stream, pre, post);
+    case 5: return launch_batched_t<5>(in, out, batch, stw, inverse, stream, pre, post);
+    case 6: return launch_batched_t<6>(in, out, batch, stw, inverse, stream, pre, post);
+    case 7: return launch_batched_t<7>(in, out, batch, stw, inverse, stream, pre, post);
+    case 8: return launch_batched_t<8>(in, out, batch, stw, inverse, stream, pre, post);
+    case 9: return launch_batched_t<9>(in, out, batch, stw, inverse, stream, pre, post);
+    case 10: return launch_batched_t<10>(in, out, batch, stw, inverse, stream, pre, post);
+    case 11: return launch_batched_t<11>(in, out, batch, stw, inverse, stream, pre, post);
+    case 12: return launch_batched_t<12>(in, out, batch, stw, inverse, stream, pre, post);
+    case 13: return launch_batched_t<13>(in, out, batch, stw, inverse, stream, pre, post);
+    case 14: return launch_batched_t<14>(in, out, batch, stw, inverse, stream, pre, post);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -172,11 +186,11 @@ bool pass_tile_supported(int log_l, int log_c) {
            (log_c >= 2 || (log_c == 1 && log_l >= 10));
 }
 
-template <int LOG_L, int LOG_C, int MODE>
-static cudaError_t launch_pass_t(const PassArgs& a, int batch, cudaStream_t stream) {
+template <int LOG_L, int LOG_C, int MODE, bool W>
+static cudaError_t launch_pass_w(const PassArgs& a, int batch, cudaStream_t stream) {
     constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
     constexpr int SMEM = pass_smem_bytes(LOG_L, LOG_C, MODE);
-    auto kernel = k_pass<LOG_L, LOG_C, MODE>;
+    auto kernel = k_pass<LOG_L, LOG_C, MODE, W>;
     static cudaError_t attr = set_smem(kernel, SMEM);
     if (attr != cudaSuccess) return attr;
     unsigned cols = 1u << (a.log2n - LOG_L);
@@ -192,6 +206,15 @@ static cudaError_t launch_pass_t(const PassArgs& a, int batch, cudaStream_t stre
         batch -= now;
     }
     return cudaGetLastError();
+}
+
+// The weighted kernel only where a weight applies: the first pass's input, the last pass's output.
+template <int LOG_L, int LOG_C, int MODE>
+static cudaError_t launch_pass_t(const PassArgs& a, int batch, cudaStream_t stream) {
+    if constexpr (MODE != 1) {
+        if (MODE == 0 ? a.pre != nullptr : a.post != nullptr) return launch_pass_w<LOG_L, LOG_C, MODE, true>(a, batch, stream);
+    }
+    return launch_pass_w<LOG_L, LOG_C, MODE, false>(a, batch, stream);
 }
 
 template <int LOG_L, int MODE>

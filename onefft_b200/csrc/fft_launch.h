@@ -30,6 +30,10 @@ struct PassArgs {
     unsigned inner_base;
     unsigned ntiles;  // grid size of the launch (tiles per transform)
     unsigned* err;    // plan's error word (mapped host memory): set by a kernel whose bounded wait ran out
+    // pointwise weights (n complex values, NULL = none): the first pass multiplies input element
+    // i by pre[i], the last pass output element i (natural order) by post[i]
+    const float2* pre;
+    const float2* post;
 };
 
 // Largest size handled by one kernel (k_tiny / k_batched).
@@ -39,8 +43,10 @@ int batched_log_c(int log_l);
 int pass_log_c(int log_l);
 bool pass_tile_supported(int log_l, int log_c);
 
+// pre / post: optional pointwise weights of the input and output (n complex values each)
 cudaError_t launch_single_kernel(int log2n, const float2* in, float2* out, long long batch, const float2* stw,
-                                 int inverse, cudaStream_t stream);
+                                 int inverse, cudaStream_t stream, const float2* pre = nullptr,
+                                 const float2* post = nullptr);
 cudaError_t launch_pass(int mode, int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t stream);
 // TMA-staged passes (fft_tma.cu): same arithmetic as launch_pass; 16-byte aligned buffers,
 // batch <= 65535, shapes pass_tma_supported()

@@ -80,18 +80,31 @@ __host__ __device__ constexpr int pass_smem_bytes(int log_l, int log_c, int mode
 
 // ---- n <= 8: one transform per thread -------------------------------------------------------------
 
-template <int LOG_N>
-__device__ __forceinline__ void tiny_transform(const float2* __restrict__ src, float2* __restrict__ dst, int inverse) {
+// W: pointwise weights of the input and output (either pointer NULL), out = post * T(pre * in);
+// without W the weights are not compiled in at all.
+template <int LOG_N, bool W = false>
+__device__ __forceinline__ void tiny_transform(const float2* __restrict__ src, float2* __restrict__ dst, int inverse,
+                                               const float2* __restrict__ pre = nullptr,
+                                               const float2* __restrict__ post = nullptr) {
     constexpr int N = 1 << LOG_N;
     float2 a[N];
 #pragma unroll
     for (int i = 0; i < N; ++i) {
         a[i] = __ldg(src + i);
+        if constexpr (W) {
+            if (pre) a[i] = cmul(a[i], __ldg(pre + i));
+        }
         if (inverse) a[i] = swap_ri(a[i]);
     }
     dft<N>(a);
 #pragma unroll
-    for (int i = 0; i < N; ++i) dst[i] = inverse ? swap_ri(a[i]) : a[i];
+    for (int i = 0; i < N; ++i) {
+        float2 y = inverse ? swap_ri(a[i]) : a[i];
+        if constexpr (W) {
+            if (post) y = cmul(y, __ldg(post + i));
+        }
+        dst[i] = y;
+    }
 }
 
 // ---- one block of whole transforms, n = 16 .. 2^14 --------------------------------------------------
@@ -99,10 +112,12 @@ __device__ __forceinline__ void tiny_transform(const float2* __restrict__ src, f
 // 2^LOG_C transforms of length L = 2^LOG_L, 16 values per thread, thread tid owns column
 // c = tid / (L/16) and butterfly lane j = tid mod (L/16). src / dst point at this thread's
 // transform; inactive columns (past the end of a batch) compute on zeros and store nothing.
-// TC selects the split-BF16 tensor-core stages (fft_tc.cuh).
-template <int LOG_L, int LOG_C, bool TC = false>
+// TC selects the split-BF16 tensor-core stages (fft_tc.cuh). W, pre, post as tiny_transform.
+template <int LOG_L, int LOG_C, bool TC = false, bool W = false>
 __device__ __forceinline__ void batched_tile(const float2* __restrict__ src, float2* __restrict__ dst, bool active,
-                                             int inverse, const float2* __restrict__ stw, float2* smem, int tid) {
+                                             int inverse, const float2* __restrict__ stw, float2* smem, int tid,
+                                             const float2* __restrict__ pre = nullptr,
+                                             const float2* __restrict__ post = nullptr) {
     constexpr int L = 1 << LOG_L, T = L / 16;
     const int j = tid & (T - 1);
     const int c = tid >> (LOG_L - 4);
@@ -112,13 +127,22 @@ __device__ __forceinline__ void batched_tile(const float2* __restrict__ src, flo
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
         float2 x = active ? ld_stream(src + T * k) : make_float2(0.f, 0.f);
+        if constexpr (W) {
+            if (pre) x = cmul(x, __ldg(pre + j + T * k));
+        }
         v[k] = inverse ? swap_ri(x) : x;
     }
     if constexpr (TC) tile_fft_tc<LOG_L, LOG_C, 1>(v, j, stw, smem, c << LOG_L, tid);
     else tile_fft<LOG_L, 1>(v, j, stw, smem, c << LOG_L);
     if (active) {
 #pragma unroll
-        for (int k = 0; k < 16; ++k) dst[T * k] = inverse ? swap_ri(v[k]) : v[k];
+        for (int k = 0; k < 16; ++k) {
+            float2 y = inverse ? swap_ri(v[k]) : v[k];
+            if constexpr (W) {
+                if (post) y = cmul(y, __ldg(post + j + T * k));
+            }
+            dst[T * k] = y;
+        }
     }
 }
 
@@ -129,7 +153,9 @@ __device__ __forceinline__ void batched_tile(const float2* __restrict__ src, flo
 // MODE 2: last pass, in place on out, no twiddle.
 // Tile t covers 2^LOG_C adjacent columns of the transform at element offset `toff`; tid runs
 // over the 2^LOG_C L / 16 threads of the tile.
-template <int LOG_L, int LOG_C, int MODE, bool TC = false>
+// W: the first pass multiplies its input by a.pre, the last pass its output by a.post (see
+// PassArgs); without W they are not compiled in.
+template <int LOG_L, int LOG_C, int MODE, bool TC = false, bool W = false>
 __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long long toff, float2* smem, int tid) {
     constexpr int L = 1 << LOG_L, T = L / 16, C = 1 << LOG_C;
     const int c = tid & (C - 1);
@@ -167,6 +193,9 @@ __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long lo
             // The first pass streams the input, which is never read again. Later passes read
             // and write `out` in place, so they avoid the read-only cache path.
             float2 x = MODE == 0 ? ld_stream(p0 + k * estep) : p0[k * estep];
+            if constexpr (W && MODE == 0) {
+                if (a.pre) x = cmul(x, __ldg(a.pre + (off0 - toff) + k * estep));
+            }
             v[k] = a.swap_in ? swap_ri(x) : x;
         }
     }
@@ -205,6 +234,9 @@ __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long lo
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
             float2 x = a.swap_out ? swap_ri(v[k]) : v[k];
+            if constexpr (W && MODE == 2) {
+                if (a.post) x = cmul(x, __ldg(a.post + (off0 - toff) + k * estep));
+            }
             if (MODE == 1 && a.l2_keep) st_policy(p0 + k * estep, x, keep);
             else p0[k * estep] = x;
         }

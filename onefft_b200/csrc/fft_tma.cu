@@ -126,7 +126,9 @@ constexpr int tma_min_blocks() {
 // One tile per block; MODE as k_pass. `tin` maps the pass's input, `tout` its output (MODE 1/2:
 // the same array, in place). Shared memory: the tile (dense as the copy lands, then reused
 // padded by the exchanges), the inter-pass twiddle factors, the mbarrier.
-template <int LOG_L, int LOG_C, int MODE>
+// W: the first pass multiplies its input by a.pre, the last pass its output by a.post
+// (instantiated only for weighted calls).
+template <int LOG_L, int LOG_C, int MODE, bool W>
 __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_L, LOG_C, MODE>()))
     k_pass_tma(PassArgs a, const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout) {
     constexpr int L = 1 << LOG_L, T = L / 16, C = 1 << LOG_C;
@@ -182,6 +184,10 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
         float2 x = smem[(j + T * k) * C + c];
+        // input element col0 + c + (j + T k) S of the transform (first pass only)
+        if constexpr (W && MODE == 0) {
+            if (a.pre) x = cmul(x, __ldg(a.pre + col0 + c + ((unsigned)(j + T * k) << a.log_s)));
+        }
         v[k] = a.swap_in ? swap_ri(x) : x;
     }
     __syncthreads();  // the dense tile is consumed; the exchanges reuse its memory
@@ -217,7 +223,16 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_
     } else {
         // dense tile back in shared memory, then one bulk tensor store
 #pragma unroll
-        for (int k = 0; k < 16; ++k) smem[(j + T * k) * C + c] = a.swap_out ? swap_ri(v[k]) : v[k];
+        for (int k = 0; k < 16; ++k) {
+            float2 x = a.swap_out ? swap_ri(v[k]) : v[k];
+            // output element q0 + c + (j + T k) S + h L S of the transform, natural order (last pass)
+            if constexpr (W && MODE == 2) {
+                if (a.post)
+                    x = cmul(x, __ldg(a.post + (unsigned)(q0 + c) + ((unsigned)(j + T * k) << a.log_s) +
+                                     ((unsigned)h << (a.log_s + LOG_L))));
+            }
+            smem[(j + T * k) * C + c] = x;
+        }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
@@ -271,11 +286,11 @@ static bool make_map(CUtensorMap* m, const float2* base, int mode, int log2n, in
     return r == CUDA_SUCCESS;
 }
 
-template <int LOG_L, int LOG_C, int MODE>
-static cudaError_t launch_tma_t(const PassArgs& a, int batch, cudaStream_t stream) {
+template <int LOG_L, int LOG_C, int MODE, bool W>
+static cudaError_t launch_tma_w(const PassArgs& a, int batch, cudaStream_t stream) {
     constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
     constexpr int SMEM = smem_bytes(LOG_L, LOG_C) + (int)sizeof(float2) * (17 * (1 << LOG_C) + 2) + 16;
-    auto kernel = k_pass_tma<LOG_L, LOG_C, MODE>;
+    auto kernel = k_pass_tma<LOG_L, LOG_C, MODE, W>;
     static cudaError_t attr =
         SMEM > 48 * 1024 ? cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) : cudaSuccess;
     if (attr != cudaSuccess) return attr;
@@ -292,31 +307,47 @@ static cudaError_t launch_tma_t(const PassArgs& a, int batch, cudaStream_t strea
     return cudaGetLastError();
 }
 
-// Tile shapes with a TMA kernel: widths 2 .. 16 columns (16-byte minimum row segment), up to
-// 8192 values per tile.
+// Tile shapes with a TMA kernel (the only ones pass_tma_supported accepts): widths 2 .. 16
+// columns (16-byte minimum row segment), up to 8192 values per tile.
+#define OFB_TMA_SHAPES(X) \
+    X(12, 1)              \
+    X(11, 1)              \
+    X(11, 2)              \
+    X(10, 1)              \
+    X(10, 2)              \
+    X(10, 3)              \
+    X(9, 2)               \
+    X(9, 3)               \
+    X(9, 4)               \
+    X(8, 2)               \
+    X(8, 3)               \
+    X(8, 4)               \
+    X(7, 3)               \
+    X(7, 4)               \
+    X(6, 4)
+
 bool pass_tma_supported(int log_l, int log_c) {
-    return log_l >= 6 && log_l <= 12 && log_c >= 1 && log_c <= 4 && log_l + log_c <= 13;
+#define OFB_TMA_MATCH(LL, LC) \
+    if (log_l == LL && log_c == LC) return true;
+    OFB_TMA_SHAPES(OFB_TMA_MATCH)
+#undef OFB_TMA_MATCH
+    return false;
+}
+
+// The weighted kernel only where a weight applies: the first pass's input, the last pass's output.
+template <int LOG_L, int LOG_C, int MODE>
+static cudaError_t launch_tma_t(const PassArgs& a, int batch, cudaStream_t stream) {
+    if constexpr (MODE != 1) {
+        if (MODE == 0 ? a.pre != nullptr : a.post != nullptr) return launch_tma_w<LOG_L, LOG_C, MODE, true>(a, batch, stream);
+    }
+    return launch_tma_w<LOG_L, LOG_C, MODE, false>(a, batch, stream);
 }
 
 template <int MODE>
 static cudaError_t launch_tma_mode(int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t s) {
 #define OFB_TMA_CASE(LL, LC) \
     if (log_l == LL && log_c == LC) return launch_tma_t<LL, LC, MODE>(a, batch, s);
-    OFB_TMA_CASE(12, 1)
-    OFB_TMA_CASE(11, 1)
-    OFB_TMA_CASE(11, 2)
-    OFB_TMA_CASE(10, 1)
-    OFB_TMA_CASE(10, 2)
-    OFB_TMA_CASE(10, 3)
-    OFB_TMA_CASE(9, 2)
-    OFB_TMA_CASE(9, 3)
-    OFB_TMA_CASE(9, 4)
-    OFB_TMA_CASE(8, 2)
-    OFB_TMA_CASE(8, 3)
-    OFB_TMA_CASE(8, 4)
-    OFB_TMA_CASE(7, 3)
-    OFB_TMA_CASE(7, 4)
-    OFB_TMA_CASE(6, 4)
+    OFB_TMA_SHAPES(OFB_TMA_CASE)
 #undef OFB_TMA_CASE
     return cudaErrorInvalidValue;
 }

@@ -361,13 +361,15 @@ extern "C" unsigned long long onefft_debug_launch_count(void) { return g_launche
 // ---- execution on device memory ---------------------------------------------------------------
 
 // Enqueues `batch` transforms; d_in / d_out are 8-byte aligned device pointers, not overlapping.
+// pre / post: optional pointwise weights (n complex values) applied by the kernel that reads the
+// input and by the one that writes the output; split-BF16 plans take none (callers check).
 static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *out, long long batch, int inverse,
-                                cudaStream_t s) {
+                                cudaStream_t s, const float2 *pre = nullptr, const float2 *post = nullptr) {
     if (batch <= 0) return cudaSuccess;
     if (p->npass == 1) {
         g_launches.fetch_add(1);
         if (p->tc) return launch_single_kernel_tc(p->log2n, in, out, batch, p->stw[0], inverse, s);
-        return launch_single_kernel(p->log2n, in, out, batch, p->stw[0], inverse, s);
+        return launch_single_kernel(p->log2n, in, out, batch, p->stw[0], inverse, s, pre, post);
     }
     PassArgs a{};
     a.log2n = p->log2n;
@@ -377,6 +379,8 @@ static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *
     a.l2_keep = p->l2_keep;
     a.tli = 31;
     a.err = p->err;
+    a.pre = pre;
+    a.post = post;
     // pass i through its TMA kernel where the plan asks for it and the shape and buffers allow
     const bool use_tma = p->tma && !p->tc && batch <= 65535 && ((((uintptr_t)in | (uintptr_t)out) & 15) == 0);
     auto run = [&](int mode, int i, const PassArgs &x) {
@@ -469,7 +473,7 @@ static bool ranges_overlap(const void *a, const void *b, size_t bytes) {
 }
 
 static int dev_batched(const onefft_plan *p, const float *d_in, float *d_out, size_t batch, int inverse,
-                       void *stream) {
+                       void *stream, const float *d_pre = nullptr, const float *d_post = nullptr) {
     t_last_error.clear();
     if (!p) return set_error(ONEFFT_ERR_ARG, "NULL plan");
     if (batch == 0) return 0;
@@ -478,8 +482,17 @@ static int dev_batched(const onefft_plan *p, const float *d_in, float *d_out, si
     if (batch > ((size_t)1 << 40) / p->n) return set_error(ONEFFT_ERR_ARG, "batch too large");
     size_t bytes = batch * p->n * sizeof(float2);
     if (ranges_overlap(d_in, d_out, bytes)) return set_error(ONEFFT_ERR_ARG, "input and output overlap");
+    if (d_pre || d_post) {
+        if (p->tc) return set_error(ONEFFT_ERR_ARG, "pointwise weights need an FP32 plan");
+        if (((uintptr_t)d_pre | (uintptr_t)d_post) & 7) return set_error(ONEFFT_ERR_ARG, "weights must be 8-byte aligned");
+        // the weights are read while the output is written: they may not share bytes with it
+        const uintptr_t o = (uintptr_t)d_out, wb = p->n * sizeof(float2);
+        for (const float *w : {d_pre, d_post})
+            if (w && (uintptr_t)w < o + bytes && o < (uintptr_t)w + wb)
+                return set_error(ONEFFT_ERR_ARG, "weights overlap the output");
+    }
     cudaError_t e = plan_enqueue(p, (const float2 *)d_in, (float2 *)d_out, (long long)batch, inverse,
-                                 (cudaStream_t)stream);
+                                 (cudaStream_t)stream, (const float2 *)d_pre, (const float2 *)d_post);
     if (e != cudaSuccess) return cuda_error(e, "kernel launch");
     return 0;
 }
@@ -492,6 +505,16 @@ extern "C" int onefft_dev_forward_batched(const onefft_plan *plan, const float *
 extern "C" int onefft_dev_inverse_batched(const onefft_plan *plan, const float *d_in, float *d_out, size_t batch,
                                           void *stream) {
     return dev_batched(plan, d_in, d_out, batch, 1, stream);
+}
+
+extern "C" int onefft_dev_forward_weighted(const onefft_plan *plan, const float *d_in, float *d_out, size_t batch,
+                                           const float *d_pre, const float *d_post, void *stream) {
+    return dev_batched(plan, d_in, d_out, batch, 0, stream, d_pre, d_post);
+}
+
+extern "C" int onefft_dev_inverse_weighted(const onefft_plan *plan, const float *d_in, float *d_out, size_t batch,
+                                           const float *d_pre, const float *d_post, void *stream) {
+    return dev_batched(plan, d_in, d_out, batch, 1, stream, d_pre, d_post);
 }
 
 extern "C" int onefft_dev_adjoint_batched(const onefft_plan *plan, const float *d_grad_out, float *d_grad_in,
