@@ -74,15 +74,16 @@ __global__ void __launch_bounds__(256) k_tiny(const float2* __restrict__ in, flo
     tiny_transform<LOG_N, W>(in + (g << LOG_N), out + (g << LOG_N), inverse, pre, post);
 }
 
-template <int LOG_L, int LOG_C, bool W>
+// INV: the direction as a compile-time constant (the re/im exchanges on load and store then
+// cost nothing in the forward kernel and no selects in the inverse one).
+template <int LOG_L, int LOG_C, bool W, int INV>
 __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4))
     k_batched(const float2* __restrict__ in, float2* __restrict__ out, long long batch,
-              const float2* __restrict__ stw, int inverse, const float2* __restrict__ pre,
-              const float2* __restrict__ post) {
+              const float2* __restrict__ stw, const float2* __restrict__ pre, const float2* __restrict__ post) {
     extern __shared__ float2 smem[];
     const int tid = threadIdx.x;
     const long long g = ((long long)blockIdx.x << LOG_C) + (tid >> (LOG_L - 4));
-    batched_tile<LOG_L, LOG_C, false, W>(in + (g << LOG_L), out + (g << LOG_L), g < batch, inverse, stw, smem, tid,
+    batched_tile<LOG_L, LOG_C, false, W>(in + (g << LOG_L), out + (g << LOG_L), g < batch, INV, stw, smem, tid,
                                          pre, post);
 }
 
@@ -108,14 +109,16 @@ static cudaError_t launch_batched_w(const float2* in, float2* out, long long bat
     constexpr int LOG_C = LOG_L >= 12 ? 0 : 12 - LOG_L;
     constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
     constexpr int SMEM = smem_bytes(LOG_L, LOG_C);
-    auto kernel = k_batched<LOG_L, LOG_C, W>;
-    static cudaError_t attr = set_smem(kernel, SMEM);
+    auto kernel = inverse ? k_batched<LOG_L, LOG_C, W, 1> : k_batched<LOG_L, LOG_C, W, 0>;
+    static cudaError_t attr = set_smem(k_batched<LOG_L, LOG_C, W, 0>, SMEM);
+    static cudaError_t attr_inv = set_smem(k_batched<LOG_L, LOG_C, W, 1>, SMEM);
     if (attr != cudaSuccess) return attr;
+    if (attr_inv != cudaSuccess) return attr_inv;
     const long long per_block = 1ll << LOG_C;
     long long blocks = (batch + per_block - 1) / per_block;
     while (blocks > 0) {  // gridDim.x limit 2^31-1
         long long now = blocks < 0x7fffffffll ? blocks : 0x7fffffffll;
-        kernel<<<(unsigned)now, THREADS, SMEM, stream>>>(in, out, batch, stw, inverse, pre, post);
+        kernel<<<(unsigned)now, THREADS, SMEM, stream>>>(in, out, batch, stw, pre, post);
         long long done = now * per_block;
         in += done << LOG_L;
         out += done << LOG_L;
