@@ -72,8 +72,8 @@ static cudaError_t launch_loss_t(const float2* x, const float* w, float2* grad, 
     constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
     constexpr int SMEM = smem_bytes(LOG_L, LOG_C);
     auto kernel = k_power_loss_grad<LOG_L, LOG_C>;
-    static cudaError_t attr =
-        SMEM > 48 * 1024 ? cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) : cudaSuccess;
+    static std::atomic<unsigned long long> done{0};
+    const cudaError_t attr = smem_limit((const void*)kernel, SMEM, done);
     if (attr != cudaSuccess) return attr;
     const long long per_block = 1ll << LOG_C;
     long long blocks = (batch + per_block - 1) / per_block;

@@ -95,12 +95,6 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4)) k_pass(PassArgs a) {
 
 // ---- launchers -------------------------------------------------------------------------------------
 
-template <class K>
-static cudaError_t set_smem(K kernel, int bytes) {
-    if (bytes <= 48 * 1024) return cudaSuccess;
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-}
-
 int batched_log_c(int log_l) { return log_l >= 12 ? 0 : 12 - log_l; }
 
 template <int LOG_L, bool W>
@@ -110,10 +104,10 @@ static cudaError_t launch_batched_w(const float2* in, float2* out, long long bat
     constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
     constexpr int SMEM = smem_bytes(LOG_L, LOG_C);
     auto kernel = inverse ? k_batched<LOG_L, LOG_C, W, 1> : k_batched<LOG_L, LOG_C, W, 0>;
-    static cudaError_t attr = set_smem(k_batched<LOG_L, LOG_C, W, 0>, SMEM);
-    static cudaError_t attr_inv = set_smem(k_batched<LOG_L, LOG_C, W, 1>, SMEM);
+    static std::atomic<unsigned long long> done_fwd{0}, done_inv{0};
+    cudaError_t attr = inverse ? smem_limit((const void*)k_batched<LOG_L, LOG_C, W, 1>, SMEM, done_inv)
+                               : smem_limit((const void*)k_batched<LOG_L, LOG_C, W, 0>, SMEM, done_fwd);
     if (attr != cudaSuccess) return attr;
-    if (attr_inv != cudaSuccess) return attr_inv;
     const long long per_block = 1ll << LOG_C;
     long long blocks = (batch + per_block - 1) / per_block;
     while (blocks > 0) {  // gridDim.x limit 2^31-1
@@ -194,7 +188,8 @@ static cudaError_t launch_pass_w(const PassArgs& a, int batch, cudaStream_t stre
     constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
     constexpr int SMEM = pass_smem_bytes(LOG_L, LOG_C, MODE);
     auto kernel = k_pass<LOG_L, LOG_C, MODE, W>;
-    static cudaError_t attr = set_smem(kernel, SMEM);
+    static std::atomic<unsigned long long> done{0};
+    const cudaError_t attr = smem_limit((const void*)kernel, SMEM, done);
     if (attr != cudaSuccess) return attr;
     unsigned cols = 1u << (a.log2n - LOG_L);
     dim3 grid(a.ntiles ? a.ntiles : cols >> LOG_C, 1, 1);

@@ -4,7 +4,25 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 namespace ofb {
+
+// Raises a kernel's dynamic shared-memory limit to `bytes` on the calling thread's current
+// device, once per device: the attribute belongs to each device's copy of the kernel, so a process
+// that runs on several GPUs must set it on every one. `done` is the call site's own bit mask of
+// devices already set (a function-local static of the launcher). Thread-safe.
+inline cudaError_t smem_limit(const void* kernel, int bytes, std::atomic<unsigned long long>& done) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
 
 // Arguments of one pass of the multi-pass decomposition (see k_pass in fft_kernels.cu).
 struct PassArgs {

@@ -21,12 +21,6 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4)) k_pass_tc(PassArgs a
     pass_tile<LOG_L, LOG_C, MODE, true>(a, blockIdx.x, (long long)blockIdx.y << a.log2n, smem, threadIdx.x);
 }
 
-template <class K>
-static cudaError_t set_smem_tc(K kernel, int bytes) {
-    if (bytes <= 48 * 1024) return cudaSuccess;
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-}
-
 template <int LOG_L>
 static cudaError_t launch_batched_tc_t(const float2* in, float2* out, long long batch, const float2* stw, int inverse,
                                        cudaStream_t stream) {
@@ -34,7 +28,8 @@ static cudaError_t launch_batched_tc_t(const float2* in, float2* out, long long 
     constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
     constexpr int SMEM = smem_bytes(LOG_L, LOG_C);
     auto kernel = k_batched_tc<LOG_L, LOG_C>;
-    static cudaError_t attr = set_smem_tc(kernel, SMEM);
+    static std::atomic<unsigned long long> done{0};
+    const cudaError_t attr = smem_limit((const void*)kernel, SMEM, done);
     if (attr != cudaSuccess) return attr;
     const long long per_block = 1ll << LOG_C;
     long long blocks = (batch + per_block - 1) / per_block;
@@ -77,7 +72,8 @@ static cudaError_t launch_pass_tc_t(const PassArgs& a, int batch, cudaStream_t s
     constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
     constexpr int SMEM = pass_smem_bytes(LOG_L, LOG_C, MODE);
     auto kernel = k_pass_tc<LOG_L, LOG_C, MODE>;
-    static cudaError_t attr = set_smem_tc(kernel, SMEM);
+    static std::atomic<unsigned long long> done{0};
+    const cudaError_t attr = smem_limit((const void*)kernel, SMEM, done);
     if (attr != cudaSuccess) return attr;
     dim3 grid(1u << (a.log2n - LOG_L - LOG_C), 1, 1);
     PassArgs b = a;

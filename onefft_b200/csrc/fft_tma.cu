@@ -291,8 +291,8 @@ static cudaError_t launch_tma_w(const PassArgs& a, int batch, cudaStream_t strea
     constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
     constexpr int SMEM = smem_bytes(LOG_L, LOG_C) + (int)sizeof(float2) * (17 * (1 << LOG_C) + 2) + 16;
     auto kernel = k_pass_tma<LOG_L, LOG_C, MODE, W>;
-    static cudaError_t attr =
-        SMEM > 48 * 1024 ? cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM) : cudaSuccess;
+    static std::atomic<unsigned long long> done{0};
+    const cudaError_t attr = smem_limit((const void*)kernel, SMEM, done);
     if (attr != cudaSuccess) return attr;
     // MODE 0 loads from `in` and stores with plain coalesced stores (tout unused); MODE 1/2
     // load and store the same tile of `out`
