@@ -146,3 +146,53 @@ def test_config2_single_2p27(ofb, oracle):
         print(f"n=2^27: GPU vs reference relative RMS difference {d:.3g}")
         assert d < 2 * oracle.tolerance(log2n)
     plan.destroy()
+
+
+@pytest.mark.parametrize("log2n", [28, 29, 30])
+def test_max_sizes_round_trip(ofb, oracle, log2n):
+    """The largest sizes OneFFT accepts (2^28 .. 2^30; 2^30 complex values = 8 GiB per buffer),
+    through size-independent properties computed on the device in FP64: the round trip
+    inverse(forward(x)) = n x, Parseval (sum |X|^2 = n sum |x|^2) and linearity
+    F(x + 2 x') = F(x) + 2 F(x') with x' a shifted copy; at 2^28 also two bins against the FP64
+    direct DFT."""
+    T = torch()
+    n = 1 << log2n
+    g = T.Generator(device="cuda").manual_seed(log2n)
+    plan = ofb.Plan(n)
+    x = T.randn(2 * n, device="cuda", generator=g)
+    y = T.empty_like(x)
+    z = T.empty_like(x)
+    plan.dev_forward(x.data_ptr(), y.data_ptr(), 1)
+    plan.dev_inverse(y.data_ptr(), z.data_ptr(), 1)
+    T.cuda.synchronize()
+
+    def sumsq(t):  # FP64 sum of squares, in chunks to bound the temporary
+        return sum(float((c.double() ** 2).sum()) for c in t.split(1 << 28))
+
+    def diffsq(a, b, scale):
+        return sum(float(((ca.double() - scale * cb.double()) ** 2).sum()) for ca, cb in zip(a.split(1 << 28), b.split(1 << 28)))
+
+    ex, ey = sumsq(x), sumsq(y)
+    assert abs(ey - n * ex) / (n * ex) < 1e-5
+    rt = (diffsq(z, x, float(n)) / (n * n * ex)) ** 0.5
+    assert rt < 2 * oracle.tolerance(log2n), rt
+    # linearity with a second input: x shifted by 12345 values
+    x2 = T.roll(x, 2 * 12345)
+    comb = x + 2 * x2
+    del z
+    y2 = T.empty_like(x)
+    yc = T.empty_like(x)
+    plan.dev_forward(x2.data_ptr(), y2.data_ptr(), 1)
+    plan.dev_forward(comb.data_ptr(), yc.data_ptr(), 1)
+    T.cuda.synchronize()
+    lin = sum(float(((cc.double() - ca.double() - 2 * cb.double()) ** 2).sum())
+              for ca, cb, cc in zip(y.split(1 << 28), y2.split(1 << 28), yc.split(1 << 28)))
+    assert (lin / sumsq(yc)) ** 0.5 < 1e-5
+    if log2n == 28:
+        xs = x.cpu().numpy()
+        bins = [1, n // 3]
+        want = oracle.dft_bins(xs, bins)
+        got = y.view(-1, 2)[bins].cpu().numpy().reshape(-1)
+        assert np.abs(got - want).max() / np.abs(want).max() < 2e-6
+    print(f"n=2^{log2n}: passes {plan.passes()}, round trip {rt:.3g}")
+    plan.destroy()
