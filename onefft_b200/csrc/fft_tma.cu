@@ -116,12 +116,16 @@ __device__ __forceinline__ unsigned long long policy_evict_first() {
 // Blocks per SM that the register allocation must allow (0: the compiler chooses freely). Measured
 // on a B200: the last pass with 1024-value tiles of 8 columns (512 threads, 70 KB of shared
 // memory) fits 3 blocks per SM at 40 registers instead of 2 at 41, which hides more of the tile
-// copy's latency (2^27: 1.18 -> 1.13 ms); the first pass with 256-value tiles of 16 columns fits 5
-// at 48 registers (no spills) instead of 4 at 51 (2^27: ~0.6 % faster). Caps on the other shapes
-// were slower (spills, or more blocks than the copy bandwidth needs).
+// copy's latency (2^27: 1.18 -> 1.13 ms); the first pass with 256-value tiles of 16 columns and
+// the middle pass with 512-value tiles of 8 columns fit 5 at 48 registers instead of 4 at 51 / 55
+// (2^27: 1.080 -> 1.073 -> 1.060 ms). Caps on the other shapes were slower (spills, or more
+// blocks than the copy bandwidth needs).
 template <int LOG_L, int LOG_C, int MODE>
 constexpr int tma_min_blocks() {
-    return LOG_L == 10 && LOG_C == 3 && MODE == 2 ? 3 : LOG_L == 8 && LOG_C == 4 && MODE == 0 ? 5 : 0;
+    return LOG_L == 10 && LOG_C == 3 && MODE == 2 ? 3
+           : LOG_L == 8 && LOG_C == 4 && MODE == 0 ? 5
+           : LOG_L == 9 && LOG_C == 3 && MODE == 1 ? 5
+                                                   : 0;
 }
 
 // One tile per block; MODE as k_pass. `tin` maps the pass's input, `tout` its output (MODE 1/2:
