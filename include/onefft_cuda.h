@@ -132,6 +132,11 @@ typedef struct onefft_uneven onefft_uneven;
  * builds the tables of every size used on the current device and the launch graph. Returns
  * NULL on invalid descriptors (reason in onefft_last_error()) or on allocation failure. */
 ONEFFT_API onefft_uneven *onefft_uneven_create(const onefft_desc *desc, size_t count);
+/* As onefft_uneven_create, with the in-block split of each size 2^13 .. 2^16 given explicitly:
+ * split_choice[m] in 0 .. 2 for 13 <= m <= 16 (other entries ignored; the array has 17 entries;
+ * NULL = the tuned choices onefft_uneven_create uses). Choice 0 is the plain path's split where it
+ * has one. For the autotuner and tests. No counterpart in OneFFT. */
+ONEFFT_API onefft_uneven *onefft_uneven_create_split(const onefft_desc *desc, size_t count, const int *split_choice);
 /* NULL is allowed. */
 ONEFFT_API void onefft_uneven_destroy(onefft_uneven *batch);
 /* Complex values the descriptors span: max over i of offset + 2^log2n. */

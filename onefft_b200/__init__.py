@@ -34,7 +34,7 @@ C_SYMBOLS = (
     "onefft_dev_weighted_power_loss",
     "onefft_plan_forward_batched", "onefft_plan_inverse_batched",
     "onefft_plan_create_split", "onefft_plan_create_tiles", "onefft_plan_create_bf16x3", "onefft_plan_passes",
-    "onefft_uneven_create", "onefft_uneven_destroy", "onefft_uneven_span", "onefft_uneven_execute",
+    "onefft_uneven_create", "onefft_uneven_create_split", "onefft_uneven_destroy", "onefft_uneven_span", "onefft_uneven_execute",
     "onefft_uneven_execute_noalloc",
     "onefft_last_error", "onefft_debug_fail_alloc", "onefft_debug_twiddles", "onefft_debug_launch_count",
 )
@@ -96,6 +96,8 @@ def lib() -> ctypes.CDLL:
         f.restype = ctypes.c_int
     L.onefft_uneven_create.argtypes = [_vp, _sz]
     L.onefft_uneven_create.restype = _vp
+    L.onefft_uneven_create_split.argtypes = [_vp, _sz, ctypes.POINTER(ctypes.c_int)]
+    L.onefft_uneven_create_split.restype = _vp
     L.onefft_uneven_destroy.argtypes = [_vp]
     L.onefft_uneven_destroy.restype = None
     L.onefft_uneven_span.argtypes = [_vp]
@@ -290,14 +292,20 @@ class UnevenBatch:
     (onefft_uneven_* in include/onefft_cuda.h). `desc` is a structured array of DESC_DTYPE, or
     three sequences (log2n, inverse, offset)."""
 
-    def __init__(self, log2n, inverse=None, offset=None):
+    def __init__(self, log2n, inverse=None, offset=None, split: dict[int, int] | None = None):
+        """split: {log2 n: choice} for sizes 2^13 .. 2^16 (onefft_uneven_create_split; sizes not
+        named take choice 0); None = the tuned choices (onefft_uneven_create)."""
         if inverse is None:
             d = np.ascontiguousarray(log2n, DESC_DTYPE)
         else:
             d = np.empty(len(log2n), DESC_DTYPE)
             d["log2n"], d["inverse"], d["offset"] = log2n, inverse, offset
         self.desc = d
-        h = lib().onefft_uneven_create(d.ctypes.data, d.size)
+        if split is None:
+            h = lib().onefft_uneven_create(d.ctypes.data, d.size)
+        else:
+            choice = (ctypes.c_int * 17)(*[int(split.get(m, 0)) for m in range(17)])
+            h = lib().onefft_uneven_create_split(d.ctypes.data, d.size, choice)
         if not h:
             raise ValueError(f"invalid uneven batch: {last_error()}")
         self._h = h

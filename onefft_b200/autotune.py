@@ -7,6 +7,11 @@ For every log2 n in range it enumerates candidate shapes — two or three passes
 each as a plan (onefft_plan_create_tiles), checks its forward result against the default plan,
 times the forward transform with CUDA events (L2 flushed before every repetition), and prints
 the fastest shape per size as the C table used by onefft_api.cu (tuned_shape) plus a JSON record.
+
+    python -m onefft_b200.autotune --uneven
+
+tunes the uneven batch instead: the in-block two-pass split of each size 2^13 .. 2^16 among the
+compiled candidates (uneven.cu kSplits), printed as uneven.cu's kUnevenTunedSplit.
 """
 from __future__ import annotations
 
@@ -72,6 +77,53 @@ def time_plan(plan, x, y, reps: int, flush) -> float:
     return ts[len(ts) // 2]
 
 
+def tune_uneven(reps: int = 9) -> dict:
+    """In-block split per size 2^13 .. 2^16 of the uneven batch: for each size, 2^25 / n
+    transforms of that size (256 MiB, half of them inverse) executed with every compiled split
+    (onefft_uneven_create_split); prints the fastest choice per size as the table
+    kUnevenTunedSplit of uneven.cu. Choice 0 everywhere runs in the kernel compiled with those
+    splits inlined, any other combination in the kernel that calls the split chosen at run time,
+    so an alternative must win despite its call overhead; the tuned combination then gets a
+    kernel of its own with its splits inlined."""
+    import numpy as np
+    out = {}
+    for m in range(13, 17):
+        n = 1 << m
+        count = (1 << 25) // n
+        rng = np.random.default_rng(m)
+        log2n = np.full(count, m, np.int32)
+        inverse = (rng.random(count) < 0.5).astype(np.int32)
+        offset = np.arange(count, dtype=np.int64) * n
+        x = torch.randn(2 * n * count, device="cuda")
+        y = torch.empty_like(x)
+        times = []
+        for choice in range(3):
+            b = ofb.UnevenBatch(log2n, inverse, offset, split={m: choice})
+            ts = []
+            for r in range(reps + 2):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                b.execute(x.data_ptr(), y.data_ptr())
+                e1.record()
+                torch.cuda.synchronize()
+                if r >= 2:
+                    ts.append(e0.elapsed_time(e1) * 1e3)
+            b.destroy()
+            ts.sort()
+            times.append(ts[len(ts) // 2])
+        best = int(np.argmin(times))
+        out[m] = {"choice": best, "us": times}
+        print(f"uneven 2^{m} x {count}: " + ", ".join(f"split {c}: {t:.1f} us" for c, t in enumerate(times)) +
+              f" -> {best}", flush=True)
+        del x, y
+        torch.cuda.empty_cache()
+    table = [0] * 17
+    for m, r in out.items():
+        table[m] = r["choice"]
+    print("constexpr int kUnevenTunedSplit[4] = {" + ", ".join(str(table[m]) for m in range(13, 17)) + "};")
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--min", type=int, default=15)
@@ -81,7 +133,14 @@ def main():
     ap.add_argument("--max-candidates", type=int, default=1000)
     ap.add_argument("--tma-only", action="store_true", help="only TMA-staged variants, no chunked passes")
     ap.add_argument("--chunked-only", action="store_true", help="only TMA-staged variants with L2-resident chunks")
+    ap.add_argument("--uneven", action="store_true", help="tune the uneven batch's in-block splits instead")
     args = ap.parse_args()
+    if args.uneven:
+        res = tune_uneven()
+        if args.out:
+            with open(args.out, "w") as f:
+                json.dump(res, f, indent=1)
+        return
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     results = {}
     for m in range(args.min, args.max + 1):

@@ -68,7 +68,7 @@ cudaError_t setup(NoAllocDevice &d, int device, cudaStream_t stream) {
     for (int m = 4; m <= kUnevenMaxLog2; ++m) {
         const int passes = m <= 12 ? 1 : 2;
         for (int p = 0; p < passes; ++p) {
-            const int l = m <= 12 ? m : uneven_split(m, p);
+            const int l = m <= 12 ? m : uneven_split(m, 0, p);  // split choice 0 (args.split stays zero)
             d.args.stw[m][p] = (const float2 *)(base + off);
             if ((e = launch_stage_table((float2 *)(base + off), l, stream)) != cudaSuccess) return e;
             off = align256(off + sizeof(float2) * (size_t)stage_table_entries_host(l));
@@ -97,7 +97,7 @@ cudaError_t setup(NoAllocDevice &d, int device, cudaStream_t stream) {
     d.args.counter = d.counter;
     d.smem = uneven_smem_bytes();
     int per_sm = 0, sms = 0;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, uneven_kernel(), 256, d.smem)) != cudaSuccess)
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, uneven_kernel(nullptr), 256, d.smem)) != cudaSuccess)
         return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) return e;
     d.grid = std::max(1, per_sm * sms);
@@ -171,7 +171,7 @@ extern "C" int onefft_uneven_execute_noalloc(const onefft_desc *desc, size_t cou
         // a pageable-memory copy has read g_sorted / g_items when it returns, so the next call
         // may refill them; the GPU work itself is only enqueued
         void *params[1] = {&args};
-        e = cudaLaunchKernel(uneven_kernel(), dim3((unsigned)std::min(dev.grid, nitems)), dim3(256), params,
+        e = cudaLaunchKernel(uneven_kernel(nullptr), dim3((unsigned)std::min(dev.grid, nitems)), dim3(256), params,
                              (size_t)dev.smem, s);
     }
     if (e != cudaSuccess) return fail(ONEFFT_ERR_CUDA_BASE - (int)e, "no-allocation uneven batch failed");

@@ -835,8 +835,29 @@ extern "C" void onefft_uneven_destroy(onefft_uneven *u) {
 
 extern "C" size_t onefft_uneven_span(const onefft_uneven *u) { return u ? u->span : 0; }
 
+static onefft_uneven *uneven_create(const onefft_desc *desc, size_t count, const int *split_choice);
+
 extern "C" onefft_uneven *onefft_uneven_create(const onefft_desc *desc, size_t count) {
     t_last_error.clear();
+    int tuned[kUnevenMaxLog2 + 1];
+    for (int m = 0; m <= kUnevenMaxLog2; ++m) tuned[m] = uneven_tuned_split(m);
+    return uneven_create(desc, count, tuned);
+}
+
+extern "C" onefft_uneven *onefft_uneven_create_split(const onefft_desc *desc, size_t count,
+                                                     const int *split_choice) {
+    t_last_error.clear();
+    if (split_choice)
+        for (int m = 13; m <= kUnevenMaxLog2; ++m)
+            if (split_choice[m] < 0 || split_choice[m] >= kUnevenSplitChoices) {
+                set_error(ONEFFT_ERR_ARG, "split choice %d for 2^%d out of range", split_choice[m], m);
+                return nullptr;
+            }
+    if (!split_choice) return onefft_uneven_create(desc, count);
+    return uneven_create(desc, count, split_choice);
+}
+
+static onefft_uneven *uneven_create(const onefft_desc *desc, size_t count, const int *split_choice) {
     if (!desc || count == 0 || count > (size_t)1 << 30) {
         set_error(ONEFFT_ERR_ARG, "invalid descriptor list");
         return nullptr;
@@ -893,6 +914,8 @@ extern "C" onefft_uneven *onefft_uneven_create(const onefft_desc *desc, size_t c
         items.push_back(UnevenItem{m, (int)k, (int)i, 0});
         i += k;
     }
+    // every size's split choice, used or not: it also selects the compiled kernel (uneven_kernel)
+    for (int m = 13; m <= kUnevenMaxLog2; ++m) u->args.split[m] = split_choice[m];
     // tables of every size used: the plain single-kernel plan up to 2^12, the in-block two-pass
     // split beyond
     bool used[kUnevenMaxLog2 + 1] = {};
@@ -902,7 +925,7 @@ extern "C" onefft_uneven *onefft_uneven_create(const onefft_desc *desc, size_t c
         if (m <= 12) {
             u->plans[m] = onefft_plan_create((size_t)1 << m);
         } else {
-            const int len[2] = {uneven_split(m, 0), uneven_split(m, 1)};
+            const int len[2] = {uneven_split(m, split_choice[m], 0), uneven_split(m, split_choice[m], 1)};
             u->plans[m] = onefft_plan_create_tiles((size_t)1 << m, 2, len, nullptr, 0, 0);
         }
         if (!u->plans[m]) {
@@ -938,8 +961,8 @@ extern "C" onefft_uneven *onefft_uneven_create(const onefft_desc *desc, size_t c
     u->smem = uneven_smem_bytes();
     int per_sm = 0, sms = 0;
     if (e == cudaSuccess && u->smem > 48 * 1024)
-        e = cudaFuncSetAttribute(uneven_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, u->smem);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, uneven_kernel(), 256, u->smem);
+        e = cudaFuncSetAttribute(uneven_kernel(u->args.split), cudaFuncAttributeMaxDynamicSharedMemorySize, u->smem);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, uneven_kernel(u->args.split), 256, u->smem);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     u->grid = std::max(1, std::min(per_sm * sms, (int)items.size()));
     // graph: zero the queue counter, then the persistent launch
@@ -957,7 +980,7 @@ extern "C" onefft_uneven *onefft_uneven_create(const onefft_desc *desc, size_t c
     if (e == cudaSuccess) {
         void *params[1] = {&u->args};
         cudaKernelNodeParams kp{};
-        kp.func = (void *)uneven_kernel();
+        kp.func = (void *)uneven_kernel(u->args.split);
         kp.gridDim = dim3((unsigned)u->grid);
         kp.blockDim = dim3(256);
         kp.sharedMemBytes = (unsigned)u->smem;
@@ -985,7 +1008,7 @@ extern "C" int onefft_uneven_execute(onefft_uneven *u, const float *d_in, float 
         u->args.out = (float2 *)d_out;
         void *params[1] = {&u->args};
         cudaKernelNodeParams kp{};
-        kp.func = (void *)uneven_kernel();
+        kp.func = (void *)uneven_kernel(u->args.split);
         kp.gridDim = dim3((unsigned)u->grid);
         kp.blockDim = dim3(256);
         kp.sharedMemBytes = (unsigned)u->smem;

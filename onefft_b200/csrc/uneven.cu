@@ -17,6 +17,8 @@
 // path's tables, so results equal onefft_dev_*_batched of each transform bit for bit wherever
 // the split is the same (every size except 2^13 and 2^14, which the plain path runs as one
 // kernel of 512 / 1024 threads and the uneven kernel as two passes of 256-thread tiles).
+// The two-pass split of 2^13 .. 2^16 is one of three compiled candidates per size, picked by the
+// autotuner (kUnevenTunedSplit); the kernel is compiled once per combination it runs.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -31,34 +33,26 @@
 
 namespace ofb {
 
-// Two-pass split of the sizes handled by one block: (L0, L1) per log2 n.
-template <int M>
-struct BigSplit;
-template <>
-struct BigSplit<13> {
-    static constexpr int L0 = 7, L1 = 6;
-};
-template <>
-struct BigSplit<14> {
-    static constexpr int L0 = 7, L1 = 7;
-};
-template <>
-struct BigSplit<15> {
-    static constexpr int L0 = 8, L1 = 7;
-};
-template <>
-struct BigSplit<16> {
-    static constexpr int L0 = 8, L1 = 8;
+// Two-pass splits (L0, L1) of the sizes handled by one block, kUnevenSplitChoices per log2 n.
+// Choice 0 is the plain path's split where it has one (2^15, 2^16), so that the batch reproduces
+// the plain path bit for bit; the others are the candidates that onefft_b200/autotune.py times.
+constexpr int kSplits[4][kUnevenSplitChoices][2] = {
+    {{7, 6}, {6, 7}, {8, 5}},  // 2^13
+    {{7, 7}, {8, 6}, {6, 8}},  // 2^14
+    {{8, 7}, {7, 8}, {9, 6}},  // 2^15
+    {{8, 8}, {9, 7}, {7, 9}},  // 2^16
 };
 
-int uneven_split(int m, int pass) {
-    switch (m) {
-    case 13: return pass ? BigSplit<13>::L1 : BigSplit<13>::L0;
-    case 14: return pass ? BigSplit<14>::L1 : BigSplit<14>::L0;
-    case 15: return pass ? BigSplit<15>::L1 : BigSplit<15>::L0;
-    case 16: return pass ? BigSplit<16>::L1 : BigSplit<16>::L0;
-    default: return 0;
-    }
+// The split the batch uses per size 2^13 .. 2^16 unless told otherwise, measured by
+// `python -m onefft_b200.autotune --uneven` on a B200 (2^25 values of one size per batch, half of
+// them inverse): 2^13 (7,6) 183 us, (6,7) 216 us, (8,5) 158 us; 2^14 (7,7) 207 us, (8,6) 183 us,
+// (6,8) 227 us; 2^15 (8,7) 206 us, (7,8) 221 us, (9,6) 239 us; 2^16 (8,8) 234 us, (9,7) 277 us,
+// (7,9) 299 us.
+constexpr int kUnevenTunedSplit[4] = {2, 1, 0, 0};
+
+int uneven_split(int m, int choice, int pass) {
+    if (m < 13 || m > 16 || choice < 0 || choice >= kUnevenSplitChoices) return 0;
+    return kSplits[m - 13][choice][pass ? 1 : 0];
 }
 
 // Tile width of an in-block pass of length 2^L: 16 columns, fewer when the tile would exceed
@@ -72,17 +66,28 @@ __host__ __device__ constexpr int inblock_pass_smem(int l, int mode) {
     return (kUnevenThreads >> (l + inblock_log_c(l) - 4)) * pass_smem_bytes(l, inblock_log_c(l), mode);
 }
 
-// Both passes of one 2^M transform by one block.
-template <int M>
-__device__ __forceinline__ void big_item(const UnevenArgs& a, const onefft_desc& d, float2* smem, int tid) {
-    constexpr int L0 = BigSplit<M>::L0, L1 = BigSplit<M>::L1;
+// What the two passes of one 2^M transform take from UnevenArgs (small enough to pass by value).
+struct BigItemArgs {
+    const float2* in;
+    float2* out;
+    const double2* tw_lo;
+    const double2* tw_hi;
+    const float2* stw0;
+    const float2* stw1;
+    int lo_bits;
+    int inverse;
+};
+
+// Both passes of one 2^M transform, split 2^L0 x 2^L1, by one block.
+template <int M, int L0, int L1>
+__device__ __forceinline__ void big_item(const BigItemArgs& b, float2* smem, int tid) {
     PassArgs p{};
-    p.in = a.in + d.offset;
-    p.out = a.out + d.offset;
+    p.in = b.in;
+    p.out = b.out;
     p.log2n = M;
-    p.tw_lo = a.tw_lo[M];
-    p.tw_hi = a.tw_hi[M];
-    p.lo_bits = a.lo_bits[M];
+    p.tw_lo = b.tw_lo;
+    p.tw_hi = b.tw_hi;
+    p.lo_bits = b.lo_bits;
     p.tli = 31;
     {
         constexpr int LC = inblock_log_c(L0), TT = 1 << (L0 + LC - 4), G = kUnevenThreads / TT;
@@ -90,9 +95,9 @@ __device__ __forceinline__ void big_item(const UnevenArgs& a, const onefft_desc&
         p.log_s = M - L0;
         p.rev_b1 = L1;
         p.rev_b2 = 0;
-        p.swap_in = d.inverse;
+        p.swap_in = b.inverse;
         p.swap_out = 0;
-        p.stw = a.stw[M][0];
+        p.stw = b.stw0;
         float2* sm = smem + (tid / TT) * (pass_smem_bytes(L0, LC, 0) / (int)sizeof(float2));
         // A first-pass tile ends by reading its transposed results back from shared memory;
         // the barrier keeps the next tile's exchanges from overwriting them while slower warps
@@ -110,13 +115,42 @@ __device__ __forceinline__ void big_item(const UnevenArgs& a, const onefft_desc&
         p.in = p.out;
         p.log_s = L0;
         p.swap_in = 0;
-        p.swap_out = d.inverse;
-        p.stw = a.stw[M][1];
+        p.swap_out = b.inverse;
+        p.stw = b.stw1;
         float2* sm = smem + (tid / TT) * (pass_smem_bytes(L1, LC, 2) / (int)sizeof(float2));
 #pragma unroll 1
         for (int t = 0; t < NT; t += G) {
             pass_tile<L1, LC, 2>(p, (unsigned)(t + tid / TT), 0, sm, tid % TT);
             __syncthreads();  // as above (this pass's tiles end in registers; kept for symmetry)
+        }
+    }
+}
+
+// Any compiled split as a call, for the kernel that picks splits at run time. Inlining every
+// split into one kernel raised its spills at 64 registers from 164 to 536 bytes, even with three
+// identical splits; fixed kernels inline the one split they run.
+template <int M, int L0, int L1>
+__device__ __noinline__ void big_item_call(const BigItemArgs b, float2* smem, int tid) {
+    big_item<M, L0, L1>(b, smem, tid);
+}
+
+// One 2^M transform with split CHOICE, or, for CHOICE = kSplitAtRunTime, the split the batch
+// was created with (UnevenArgs::split).
+constexpr int kSplitAtRunTime = -1;
+
+template <int M, int CHOICE>
+__device__ __forceinline__ void big_choice(const UnevenArgs& a, const onefft_desc& d, float2* smem, int tid) {
+    constexpr int I = M - 13;
+    const BigItemArgs b{a.in + d.offset, a.out + d.offset, a.tw_lo[M], a.tw_hi[M],
+                        a.stw[M][0],     a.stw[M][1],      a.lo_bits[M], d.inverse};
+    if constexpr (CHOICE != kSplitAtRunTime) {
+        big_item<M, kSplits[I][CHOICE][0], kSplits[I][CHOICE][1]>(b, smem, tid);
+    } else {
+        static_assert(kUnevenSplitChoices == 3, "one branch per compiled split");
+        switch (a.split[M]) {
+        case 1: big_item_call<M, kSplits[I][1][0], kSplits[I][1][1]>(b, smem, tid); break;
+        case 2: big_item_call<M, kSplits[I][2][0], kSplits[I][2][1]>(b, smem, tid); break;
+        default: big_item_call<M, kSplits[I][0][0], kSplits[I][0][1]>(b, smem, tid); break;
         }
     }
 }
@@ -142,6 +176,8 @@ __device__ __forceinline__ void tiny_item(const UnevenArgs& a, const UnevenItem&
 // 20000 transforms of 2^4 .. 2^16, 1.21 ms at 2 blocks per SM (128 registers), 1.14 ms at 3
 // (80 registers), 1.12 ms at 4; items are latency-bound tile sequences, so more resident blocks
 // hide more of each block's waits.
+// C13 .. C16: the split of each size 2^13 .. 2^16 (an index into kSplits, or kSplitAtRunTime).
+template <int C13, int C14, int C15, int C16>
 __global__ void __launch_bounds__(kUnevenThreads, 4) k_uneven(UnevenArgs a) {
     extern __shared__ float2 smem[];
     __shared__ int s_item;
@@ -167,10 +203,10 @@ __global__ void __launch_bounds__(kUnevenThreads, 4) k_uneven(UnevenArgs a) {
         case 10: batch_item<10>(a, w, smem, tid); break;
         case 11: batch_item<11>(a, w, smem, tid); break;
         case 12: batch_item<12>(a, w, smem, tid); break;
-        case 13: big_item<13>(a, a.desc[w.first], smem, tid); break;
-        case 14: big_item<14>(a, a.desc[w.first], smem, tid); break;
-        case 15: big_item<15>(a, a.desc[w.first], smem, tid); break;
-        case 16: big_item<16>(a, a.desc[w.first], smem, tid); break;
+        case 13: big_choice<13, C13>(a, a.desc[w.first], smem, tid); break;
+        case 14: big_choice<14, C14>(a, a.desc[w.first], smem, tid); break;
+        case 15: big_choice<15, C15>(a, a.desc[w.first], smem, tid); break;
+        case 16: big_choice<16, C16>(a, a.desc[w.first], smem, tid); break;
         default: break;
         }
         __syncthreads();  // the next item may reuse shared memory
@@ -179,13 +215,31 @@ __global__ void __launch_bounds__(kUnevenThreads, 4) k_uneven(UnevenArgs a) {
 
 int uneven_smem_bytes() {
     int s = smem_bytes(12, 0);
-    for (int m = 13; m <= 16; ++m) {
-        s = std::max(s, inblock_pass_smem(uneven_split(m, 0), 0));
-        s = std::max(s, inblock_pass_smem(uneven_split(m, 1), 2));
-    }
+    for (int m = 13; m <= 16; ++m)
+        for (int c = 0; c < kUnevenSplitChoices; ++c) {
+            s = std::max(s, inblock_pass_smem(uneven_split(m, c, 0), 0));
+            s = std::max(s, inblock_pass_smem(uneven_split(m, c, 1), 2));
+        }
     return s;
 }
 
-const void *uneven_kernel() { return (const void *)k_uneven; }
+// The compiled kernels: every split inlined for the plain path's splits (choice 0 everywhere)
+// and for the tuned choices, and one that reads the choices from its arguments (any other
+// combination; the autotuner times candidates with it).
+int uneven_tuned_split(int m) { return m >= 13 && m <= 16 ? kUnevenTunedSplit[m - 13] : 0; }
+
+const void *uneven_kernel(const int *split) {
+    bool plain = true, tuned = true;
+    for (int m = 13; m <= kUnevenMaxLog2; ++m) {
+        const int c = split ? split[m] : 0;
+        plain = plain && c == 0;
+        tuned = tuned && c == kUnevenTunedSplit[m - 13];
+    }
+    if (plain) return (const void *)k_uneven<0, 0, 0, 0>;
+    if (tuned)
+        return (const void *)k_uneven<kUnevenTunedSplit[0], kUnevenTunedSplit[1], kUnevenTunedSplit[2],
+                                      kUnevenTunedSplit[3]>;
+    return (const void *)k_uneven<kSplitAtRunTime, kSplitAtRunTime, kSplitAtRunTime, kSplitAtRunTime>;
+}
 
 }  // namespace ofb

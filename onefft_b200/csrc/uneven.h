@@ -9,6 +9,7 @@
 namespace ofb {
 
 constexpr int kUnevenMaxLog2 = 16;
+constexpr int kUnevenSplitChoices = 3;  // compiled two-pass splits per size 2^13 .. 2^16
 
 // One work item: `count` transforms of size 2^log2n at desc[first .. first + count).
 struct UnevenItem {
@@ -30,12 +31,17 @@ struct UnevenArgs {
     const double2 *tw_lo[kUnevenMaxLog2 + 1];
     const double2 *tw_hi[kUnevenMaxLog2 + 1];
     int lo_bits[kUnevenMaxLog2 + 1];
+    int split[kUnevenMaxLog2 + 1];  // 2^13 .. 2^16: which compiled split (0 .. kUnevenSplitChoices - 1)
 };
 
-// Pass lengths (log2) of the two in-block passes for 13 <= m <= 16.
-int uneven_split(int m, int pass);
-// Dynamic shared memory of k_uneven, and the kernel itself (for graph nodes / occupancy).
+// Pass lengths (log2) of the two in-block passes of split `choice` for 13 <= m <= 16 (0 for other
+// m or choices).
+int uneven_split(int m, int choice, int pass);
+// The autotuned split choice of size 2^m (0 outside 13 .. 16).
+int uneven_tuned_split(int m);
+// Dynamic shared memory of k_uneven, and the kernel that runs split choices split[13 .. 16]
+// (NULL: choice 0 everywhere), for graph nodes / launches / occupancy.
 int uneven_smem_bytes();
-const void *uneven_kernel();
+const void *uneven_kernel(const int *split);
 
 }  // namespace ofb

@@ -150,6 +150,38 @@ def test_uneven_in_block_passes_repeatable(ofb, oracle):
     batch.destroy()
 
 
+@pytest.mark.parametrize("choice", [0, 1, 2])
+def test_uneven_split_choices(ofb, oracle, choice):
+    """Every compiled in-block split of 2^13 .. 2^16 (onefft_uneven_create_split), at 8-byte
+    aligned offsets: within twice the size's error bound of the plain path, within the bound of
+    FP64 on sampled transforms, and two executions equal bit for bit."""
+    T = torch()
+    rng = np.random.default_rng(40 + choice)
+    log2n = rng.integers(13, 17, 200).astype(np.int32)
+    inverse = (rng.random(log2n.size) < 0.5).astype(np.int32)
+    sizes = (1 << log2n.astype(np.int64)) + 1
+    offset = np.concatenate([[1], 1 + np.cumsum(sizes)[:-1]]).astype(np.int64)
+    span = int(offset[-1] + (1 << int(log2n[-1])))
+    x, _ = oracle.gen_uniform(2 * span, 41 + choice)
+    batch = ofb.UnevenBatch(log2n, inverse, offset, split={m: choice for m in range(13, 17)})
+    d_in = T.from_numpy(x).cuda()
+    got = T.zeros_like(d_in)
+    batch.execute(d_in.data_ptr(), got.data_ptr())
+    again = T.zeros_like(d_in)
+    batch.execute(d_in.data_ptr(), again.data_ptr())
+    T.cuda.synchronize()
+    assert T.equal(again, got)
+    want = plain_path(ofb, T, log2n, inverse, offset, d_in)
+    compare(oracle, log2n, offset, got, want, tol_sizes=(13, 14, 15, 16))
+    g = got.cpu().numpy()
+    for i in rng.choice(len(log2n), 8, replace=False):
+        m, off, inv = int(log2n[i]), int(offset[i]), bool(inverse[i])
+        n = 1 << m
+        want64 = oracle.fft64_numpy(x[2 * off:2 * (off + n)], inv)
+        assert oracle.rel_rms(g[2 * off:2 * (off + n)], want64) < oracle.tolerance(m)
+    batch.destroy()
+
+
 def test_uneven_rejects_bad_arguments(ofb):
     T = torch()
     L = ofb.lib()
@@ -162,3 +194,6 @@ def test_uneven_rejects_bad_arguments(ofb):
     assert L.onefft_uneven_execute(b._h, buf.data_ptr() + 4, buf.data_ptr() + 512, None) == -2
     assert L.onefft_uneven_execute(b._h, buf.data_ptr(), buf.data_ptr() + 64, None) == -2  # overlap
     b.destroy()
+    for bad in (-1, 3):
+        with pytest.raises(ValueError):
+            ofb.UnevenBatch([14], [0], [0], split={14: bad})
