@@ -134,7 +134,15 @@ static const Shape kTuned[] = {
     /* 25 */ {3, {8, 8, 9}, {3, 3, 3}, 0, 0, 1},
     /* 26 */ {3, {8, 8, 10}, {3, 3, 3}, 0, 0, 1},
     /* 27 */ {3, {8, 9, 10}, {4, 3, 3}, 0, 0, 1},
+    // 2^28 .. 2^30 (one 2^30 transform holds 16 GiB of buffers), timed among three-pass splits
+    // with default tile widths: 2^28 (10,10,8) 2.57 ms against (10,9,9) 2.62; 2^29 (10,10,9)
+    // 5.28 ms, the fastest of six; 2^30 (10,11,9) 11.2 ms against 12.6-16.2 ms for seven others,
+    // (10,10,10) 12.9 ms.
+    /* 28 */ {3, {10, 10, 8}, {3, 3, 4}, 1, 0, 1},
+    /* 29 */ {3, {10, 10, 9}, {3, 3, 4}, 1, 0, 1},
+    /* 30 */ {3, {10, 11, 9}, {3, 2, 4}, 1, 0, 1},
 };
+static_assert(sizeof(kTuned) / sizeof(kTuned[0]) == 30 - 15 + 1, "one shape per size 2^15 .. 2^30");
 
 static Shape tuned_shape(int m) {
     Shape s{};
@@ -143,21 +151,7 @@ static Shape tuned_shape(int m) {
         s.len[0] = m;
         return s;
     }
-    if (m >= 15 && m <= 27) return kTuned[m - 15];
-    if (m <= 24) {
-        s.npass = 2;
-        s.len[0] = (m + 1) / 2;
-        s.len[1] = m / 2;
-    } else {
-        s.npass = 3;
-        s.len[0] = (m + 2) / 3;
-        s.len[1] = (m + 1) / 3;
-        s.len[2] = m / 3;
-    }
-    for (int i = 0; i < s.npass; ++i) s.cols[i] = pass_log_c(s.len[i]);
-    s.l2_keep = 1;
-    s.tma = 1;  // passes whose tile shape has a TMA kernel use it (as the tuned large sizes do)
-    return s;
+    return kTuned[m - 15];
 }
 
 static bool valid_shape(int m, const Shape &s) {
