@@ -107,6 +107,16 @@ def test_uneven_descriptors_validated_on_host(cuda_lib):
         assert cuda_lib.onefft_uneven_create(d.ctypes.data, d.size) is None
         assert cuda_lib.onefft_last_error()
     assert cuda_lib.onefft_uneven_create(None, 3) is None
+    # split choices outside the compiled candidates (0 .. 2 per size 2^13 .. 2^16)
+    d = np.empty(1, ofb.DESC_DTYPE)
+    d["log2n"], d["inverse"], d["offset"] = 14, 0, 0
+    for m, bad_choice in ((13, 3), (16, -1)):
+        choice = (ctypes.c_int * 17)()
+        choice[m] = bad_choice
+        assert cuda_lib.onefft_uneven_create_split(d.ctypes.data, 1, choice) is None
+        assert b"split choice" in cuda_lib.onefft_last_error()
+    with pytest.raises(ValueError):
+        ofb.UnevenBatch([17], [0], [0], split={13: 1})
     cuda_lib.onefft_uneven_destroy(None)
     assert cuda_lib.onefft_uneven_span(None) == 0
     assert cuda_lib.onefft_uneven_execute(None, 0, 0, None) == -2
