@@ -190,14 +190,16 @@ def run_reference(args, rank: int):
     """--impl reference: the reference CPU library on this host, rank 0 only."""
     if rank != 0:
         return
+    # a step is ~1-1.5 s of host work: at most 5 timed and 3 warm-up steps keep the run short
     steps = max(1, min(args.steps, 5))
-    times, cores, kind, impl = cpu_step_times(steps, 1)
+    warmup = max(1, min(args.warmup, 3))
+    times, cores, kind, impl = cpu_step_times(steps, warmup)
     t = sum(times) / len(times)
     value = STEP_FLOPS / t / 1e9
-    sample = (f"the whole step per timed step ({steps} steps after 1 warm-up; {impl} kernels, "
+    sample = (f"the whole step per timed step ({steps} steps after {warmup} warm-up; {impl} kernels, "
               f"{cores} threads, largest transforms first)")
     line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": steps,
-            "warmup": 1, "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
+            "warmup": warmup, "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
             "config": dict(WORKLOAD, parallelism="host threads"),
             "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": cores, "kind": kind, "sample": sample},
