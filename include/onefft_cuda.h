@@ -87,7 +87,10 @@ ONEFFT_API int onefft_plan_inverse_batched(const onefft_plan *plan, const float 
 ONEFFT_API onefft_plan *onefft_plan_create_split(size_t n, int npass, const int *log2_len);
 
 /* As onefft_plan_create_split, also choosing each pass's tile width: 2^log2_cols[p] adjacent
- * columns per thread block (1 .. 4, at most 16384 values per tile; NULL = default widths),
+ * columns per thread block (1 .. 4, at most 16384 values per tile; NULL = default widths). For
+ * npass = 1 (n = 2^4 .. 2^14), log2_cols[0] is instead the number of whole transforms per block
+ * (log2; the default 4096 / n, or half or twice that up to 8192 values; -1 or NULL = the tuned
+ * choice); results are the same bit for bit whatever the choice.
  * `options` (ONEFFT_OPT_L2_KEEP: store the array between passes with L2 evict-last priority;
  * ONEFFT_OPT_TMA: stage each pass tile through one bulk tensor copy where the tile shape has
  * such a kernel and the buffers are 16-byte aligned), and, for three passes, log2_chunk > 0 to

@@ -12,6 +12,11 @@ the fastest shape per size as the C table used by onefft_api.cu (tuned_shape) pl
 
 tunes the uneven batch instead: the in-block two-pass split of each size 2^13 .. 2^16 among the
 compiled candidates (uneven.cu kSplits), printed as uneven.cu's kUnevenTunedSplit.
+
+    python -m onefft_b200.autotune --batched
+
+tunes the one-kernel sizes 2^4 .. 2^14: whole transforms per thread block (the default 4096 / n,
+half or twice that), printed as onefft_api.cu's kBatchedTunedLogC.
 """
 from __future__ import annotations
 
@@ -77,6 +82,63 @@ def time_plan(plan, x, y, reps: int, flush) -> float:
     return ts[len(ts) // 2]
 
 
+def batched_log_c_candidates(l: int) -> list[int]:
+    """Transforms per block (log2) compiled for the one-kernel size 2^l (fft_kernels.cu,
+    batched_log_c_supported): the default 4096 / n, half and twice that up to 8192 values."""
+    b = max(0, 12 - l)
+    return [c for c in (b - 1, b, b + 1) if c == b or (c >= 0 and l + c <= 13)]
+
+
+def tune_batched(reps: int = 9) -> dict:
+    """Transforms per block of the one-kernel sizes 2^4 .. 2^14: for each size a batch of
+    2^25 / n transforms (256 MiB), forward, with every compiled width; each result must equal the
+    default's bit for bit. Prints the fastest width per size as onefft_api.cu's
+    kBatchedTunedLogC."""
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    out = {}
+    for l in range(4, 15):
+        n = 1 << l
+        batch = (1 << 25) // n
+        x = torch.randn(2 * n * batch, device="cuda")
+        ref = torch.empty_like(x)
+        y = torch.empty_like(x)
+        p0 = ofb.Plan(n, split=(l,), cols=(max(0, 12 - l),))
+        p0.dev_forward(x.data_ptr(), ref.data_ptr(), batch)
+        p0.destroy()
+        times = {}
+        for c in batched_log_c_candidates(l):
+            plan = ofb.Plan(n, split=(l,), cols=(c,))
+            y.fill_(float("nan"))
+            plan.dev_forward(x.data_ptr(), y.data_ptr(), batch)
+            torch.cuda.synchronize()
+            if not torch.equal(y, ref):
+                raise RuntimeError(f"2^{l} with 2^{c} transforms per block differs from the default")
+            ts = []
+            for r in range(reps + 2):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                plan.dev_forward(x.data_ptr(), y.data_ptr(), batch)
+                e1.record()
+                torch.cuda.synchronize()
+                if r >= 2:
+                    ts.append(e0.elapsed_time(e1) * 1e3)
+            plan.destroy()
+            ts.sort()
+            times[c] = ts[len(ts) // 2]
+        best = min(times, key=times.get)
+        out[l] = {"log_c": best, "us": times}
+        print(f"batched 2^{l} x {batch}: " + ", ".join(f"{1 << c}/block {t:.1f} us" for c, t in times.items()) +
+              f" -> {1 << best}", flush=True)
+        del x, ref, y
+        torch.cuda.empty_cache()
+    table = [-1] * 15
+    for l, r in out.items():
+        table[l] = r["log_c"]
+    print("static const int kBatchedTunedLogC[kMaxSingleLog2 + 1] = {" + ", ".join(str(v) for v in table) + "};")
+    return out
+
+
 def tune_uneven(reps: int = 9) -> dict:
     """In-block split per size 2^13 .. 2^16 of the uneven batch: for each size, 2^25 / n
     transforms of that size (256 MiB, half of them inverse) executed with every compiled split
@@ -134,9 +196,10 @@ def main():
     ap.add_argument("--tma-only", action="store_true", help="only TMA-staged variants, no chunked passes")
     ap.add_argument("--chunked-only", action="store_true", help="only TMA-staged variants with L2-resident chunks")
     ap.add_argument("--uneven", action="store_true", help="tune the uneven batch's in-block splits instead")
+    ap.add_argument("--batched", action="store_true", help="tune the transforms per block of sizes 2^4 .. 2^14")
     args = ap.parse_args()
-    if args.uneven:
-        res = tune_uneven()
+    if args.uneven or args.batched:
+        res = tune_uneven() if args.uneven else tune_batched()
         if args.out:
             with open(args.out, "w") as f:
                 json.dump(res, f, indent=1)

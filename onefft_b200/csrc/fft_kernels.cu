@@ -1,10 +1,11 @@
 // The transform kernels for sm_100a and their launchers.
 //
 //   k_tiny     n = 1, 2, 4, 8: one thread per transform, all in registers.
-//   k_batched  n = 16 .. 2^14 in one kernel: each block holds C = max(1, 4096 / n) whole
-//              transforms (C n / 16 threads, 16 values per thread), Stockham radix-16 stages in
-//              registers with exchanges through padded shared memory. Loads and stores are
-//              coalesced 8-byte accesses straight between HBM and registers.
+//   k_batched  n = 16 .. 2^14 in one kernel: each block holds C whole transforms (by default
+//              max(1, 4096 / n), or half or twice that as the plan's tuned width says; C n / 16
+//              threads, 16 values per thread), Stockham radix-16 stages in registers with
+//              exchanges through padded shared memory. Loads and stores are 8-byte accesses
+//              straight between HBM and registers, or for n <= 64 coalesced through shared memory.
 //   k_pass     n > 2^14: one pass of a two- or three-pass four-step decomposition
 //              n = L0 L1 (L2). A block transforms a tile of C adjacent columns of length Lp.
 //              Pass 0 reads the input in natural order (columns are adjacent addresses),
@@ -74,6 +75,52 @@ __global__ void __launch_bounds__(256) k_tiny(const float2* __restrict__ in, flo
     tiny_transform<LOG_N, W>(in + (g << LOG_N), out + (g << LOG_N), inverse, pre, post);
 }
 
+// The block's 2^LOG_C transforms of n = 16 .. 64 through shared memory. Each thread's 16
+// values of one transform lie T = n / 16 apart, so direct loads touch 32 / T different lines per
+// warp instruction (for n = 16 one value of each); the block's transforms are one contiguous run,
+// so it is loaded and stored with consecutive threads on consecutive values instead, in the
+// padded layout the exchanges use (transform c's value e at spad(c n + e)). Measured on a B200
+// with 2^25 values per batch and 4096-value tiles, forward: n = 16 303 -> 90 us, n = 32 162 -> 94,
+// n = 64 104 -> 96 (82 us is the copy bound of the 537 MB moved); 2048-value tiles 86-87 us.
+template <int LOG_L, int LOG_C, int INV>
+__device__ __forceinline__ void batched_tile_staged(const float2* __restrict__ in, float2* __restrict__ out,
+                                                    long long batch, const float2* __restrict__ stw, float2* smem,
+                                                    int tid) {
+    constexpr int L = 1 << LOG_L, T = L / 16, THREADS = 1 << (LOG_L + LOG_C - 4);
+    const long long g0 = (long long)blockIdx.x << LOG_C;
+    const long long left = batch - g0;
+    const int valid = (left < (1 << LOG_C) ? (int)left : (1 << LOG_C)) << LOG_L;  // values of this block
+    const float2* src = in + (g0 << LOG_L);
+    float2* dst = out + (g0 << LOG_L);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int x = tid + THREADS * i;
+        smem[spad(x)] = x < valid ? ld_stream(src + x) : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const int c = tid >> (LOG_L - 4), j = tid & (T - 1);
+    float2 v[16];
+    {
+        const float2* r = smem + spad(c * L + j);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[k] = INV ? swap_ri(r[padc(k * T)]) : r[padc(k * T)];
+    }
+    __syncthreads();  // every input is in registers before the exchanges reuse the memory
+    tile_fft<LOG_L, 1>(v, j, stw, smem, c << LOG_L);
+    __syncthreads();  // n = 16 has no exchange: other threads may still be reading inputs
+    {
+        float2* w = smem + spad(c * L + j);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) w[padc(k * T)] = INV ? swap_ri(v[k]) : v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int x = tid + THREADS * i;
+        if (x < valid) dst[x] = smem[spad(x)];
+    }
+}
+
 // INV: the direction as a compile-time constant (the re/im exchanges on load and store then
 // cost nothing in the forward kernel and no selects in the inverse one).
 template <int LOG_L, int LOG_C, bool W, int INV>
@@ -82,9 +129,13 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4))
               const float2* __restrict__ stw, const float2* __restrict__ pre, const float2* __restrict__ post) {
     extern __shared__ float2 smem[];
     const int tid = threadIdx.x;
-    const long long g = ((long long)blockIdx.x << LOG_C) + (tid >> (LOG_L - 4));
-    batched_tile<LOG_L, LOG_C, false, W>(in + (g << LOG_L), out + (g << LOG_L), g < batch, INV, stw, smem, tid,
-                                         pre, post);
+    if constexpr (LOG_L <= 6 && !W) {
+        batched_tile_staged<LOG_L, LOG_C, INV>(in, out, batch, stw, smem, tid);
+    } else {
+        const long long g = ((long long)blockIdx.x << LOG_C) + (tid >> (LOG_L - 4));
+        batched_tile<LOG_L, LOG_C, false, W>(in + (g << LOG_L), out + (g << LOG_L), g < batch, INV, stw, smem, tid,
+                                             pre, post);
+    }
 }
 
 template <int LOG_L, int LOG_C, int MODE, bool W>
@@ -95,12 +146,19 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4)) k_pass(PassArgs a) {
 
 // ---- launchers -------------------------------------------------------------------------------------
 
-int batched_log_c(int log_l) { return log_l >= 12 ? 0 : 12 - log_l; }
+constexpr int default_batched_log_c(int log_l) { return log_l >= 12 ? 0 : 12 - log_l; }
 
-template <int LOG_L, bool W>
+int batched_log_c(int log_l) { return default_batched_log_c(log_l); }
+
+bool batched_log_c_supported(int log_l, int log_c) {
+    if (log_l < 4 || log_l > kMaxSingleLog2) return false;
+    const int b = default_batched_log_c(log_l);
+    return log_c == b || (log_c >= 0 && log_c >= b - 1 && log_c <= b + 1 && log_l + log_c <= 13);
+}
+
+template <int LOG_L, bool W, int LOG_C>
 static cudaError_t launch_batched_w(const float2* in, float2* out, long long batch, const float2* stw, int inverse,
                                     cudaStream_t stream, const float2* pre, const float2* post) {
-    constexpr int LOG_C = LOG_L >= 12 ? 0 : 12 - LOG_L;
     constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
     constexpr int SMEM = smem_bytes(LOG_L, LOG_C);
     auto kernel = inverse ? k_batched<LOG_L, LOG_C, W, 1> : k_batched<LOG_L, LOG_C, W, 0>;
@@ -124,9 +182,16 @@ static cudaError_t launch_batched_w(const float2* in, float2* out, long long bat
 
 template <int LOG_L>
 static cudaError_t launch_batched_t(const float2* in, float2* out, long long batch, const float2* stw, int inverse,
-                                    cudaStream_t stream, const float2* pre, const float2* post) {
-    return pre || post ? launch_batched_w<LOG_L, true>(in, out, batch, stw, inverse, stream, pre, post)
-                       : launch_batched_w<LOG_L, false>(in, out, batch, stw, inverse, stream, nullptr, nullptr);
+                                    cudaStream_t stream, const float2* pre, const float2* post, int log_c) {
+    constexpr int B = default_batched_log_c(LOG_L);
+    if (pre || post) return launch_batched_w<LOG_L, true, B>(in, out, batch, stw, inverse, stream, pre, post);
+    if constexpr (B >= 1)
+        if (log_c == B - 1)
+            return launch_batched_w<LOG_L, false, B - 1>(in, out, batch, stw, inverse, stream, nullptr, nullptr);
+    if constexpr (LOG_L + B + 1 <= 13)
+        if (log_c == B + 1)
+            return launch_batched_w<LOG_L, false, B + 1>(in, out, batch, stw, inverse, stream, nullptr, nullptr);
+    return launch_batched_w<LOG_L, false, B>(in, out, batch, stw, inverse, stream, nullptr, nullptr);
 }
 
 template <int LOG_N>
@@ -148,24 +213,25 @@ static cudaError_t launch_tiny_t(const float2* in, float2* out, long long batch,
 }
 
 cudaError_t launch_single_kernel(int log2n, const float2* in, float2* out, long long batch, const float2* stw,
-                                 int inverse, cudaStream_t stream, const float2* pre, const float2* post) {
+                                 int inverse, cudaStream_t stream, const float2* pre, const float2* post,
+                                 int log_c) {
     if (batch <= 0) return cudaSuccess;
     switch (log2n) {
     case 0: return launch_tiny_t<0>(in, out, batch, inverse, stream, pre, post);
     case 1: return launch_tiny_t<1>(in, out, batch, inverse, stream, pre, post);
     case 2: return launch_tiny_t<2>(in, out, batch, inverse, stream, pre, post);
     case 3: return launch_tiny_t<3>(in, out, batch, inverse, stream, pre, post);
-    case 4: return launch_batched_t<4>(in, out, batch, stw, inverse, stream, pre, post);
-    case 5: return launch_batched_t<5>(in, out, batch, stw, inverse, stream, pre, post);
-    case 6: return launch_batched_t<6>(in, out, batch, stw, inverse, stream, pre, post);
-    case 7: return launch_batched_t<7>(in, out, batch, stw, inverse, stream, pre, post);
-    case 8: return launch_batched_t<8>(in, out, batch, stw, inverse, stream, pre, post);
-    case 9: return launch_batched_t<9>(in, out, batch, stw, inverse, stream, pre, post);
-    case 10: return launch_batched_t<10>(in, out, batch, stw, inverse, stream, pre, post);
-    case 11: return launch_batched_t<11>(in, out, batch, stw, inverse, stream, pre, post);
-    case 12: return launch_batched_t<12>(in, out, batch, stw, inverse, stream, pre, post);
-    case 13: return launch_batched_t<13>(in, out, batch, stw, inverse, stream, pre, post);
-    case 14: return launch_batched_t<14>(in, out, batch, stw, inverse, stream, pre, post);
+    case 4: return launch_batched_t<4>(in, out, batch, stw, inverse, stream, pre, post, log_c);
+    case 5: return launch_batched_t<5>(in, out, batch, stw, inverse, stream, pre, post, log_c);
+    case 6: return launch_batched_t<6>(in, out, batch, stw, inverse, stream, pre, post, log_c);
+    case 7: return launch_batched_t<7>(in, out, batch, stw, inverse, stream, pre, post, log_c);
+    case 8: return launch_batched_t<8>(in, out, batch, stw, inverse, stream, pre, post, log_c);
+    case 9: return launch_batched_t<9>(in, out, batch, stw, inverse, stream, pre, post, log_c);
+    case 10: return launch_batched_t<10>(in, out, batch, stw, inverse, stream, pre, post, log_c);
+    case 11: return launch_batched_t<11>(in, out, batch, stw, inverse, stream, pre, post, log_c);
+    case 12: return launch_batched_t<12>(in, out, batch, stw, inverse, stream, pre, post, log_c);
+    case 13: return launch_batched_t<13>(in, out, batch, stw, inverse, stream, pre, post, log_c);
+    case 14: return launch_batched_t<14>(in, out, batch, stw, inverse, stream, pre, post, log_c);
     default: return cudaErrorInvalidValue;
     }
 }

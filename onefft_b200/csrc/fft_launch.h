@@ -57,14 +57,20 @@ struct PassArgs {
 // Largest size handled by one kernel (k_tiny / k_batched).
 constexpr int kMaxSingleLog2 = 14;
 
+// log2 of the transforms per block of the one-kernel sizes: the default (4096-value tiles),
+// and whether a width was compiled (the default, half and twice as many transforms per block, up
+// to 8192 values; sizes 2^13 and 2^14 only one per block)
 int batched_log_c(int log_l);
+bool batched_log_c_supported(int log_l, int log_c);
 int pass_log_c(int log_l);
 bool pass_tile_supported(int log_l, int log_c);
 
-// pre / post: optional pointwise weights of the input and output (n complex values each)
+// pre / post: optional pointwise weights of the input and output (n complex values each);
+// log_c: transforms per block of k_batched (batched_log_c_supported; < 0 = the default; weighted
+// calls always use the default)
 cudaError_t launch_single_kernel(int log2n, const float2* in, float2* out, long long batch, const float2* stw,
                                  int inverse, cudaStream_t stream, const float2* pre = nullptr,
-                                 const float2* post = nullptr);
+                                 const float2* post = nullptr, int log_c = -1);
 cudaError_t launch_pass(int mode, int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t stream);
 // TMA-staged passes (fft_tma.cu): same arithmetic as launch_pass; 16-byte aligned buffers,
 // batch <= 65535, shapes pass_tma_supported()

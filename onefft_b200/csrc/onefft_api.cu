@@ -89,7 +89,8 @@ struct onefft_plan {
     int device;
     int npass;
     int len[3];            // log2 of each pass length
-    int cols[3];           // log2 of the tile width (columns per block) of each pass
+    int cols[3];           // log2 of the tile width (columns per block) of each pass; one kernel:
+                           // cols[0] = log2 of the transforms per block (-1 = default)
     int l2_keep;           // intermediate stores with L2 evict-last priority
     int chunk;             // three passes: log2 of the last-digit columns per chunk of passes 0+1 (0 = none)
     int tc;                // radix-16 stages as split-BF16 tensor-core products (onefft_plan_create_bf16x3)
@@ -144,18 +145,27 @@ static const Shape kTuned[] = {
 };
 static_assert(sizeof(kTuned) / sizeof(kTuned[0]) == 30 - 15 + 1, "one shape per size 2^15 .. 2^30");
 
+// Transforms per block (log2) of the one-kernel sizes 2^4 .. 2^14, from
+// `python -m onefft_b200.autotune --batched` on a B200 (forward, 2^25 values per batch, median of
+// 9): 2048-value tiles up to n = 2^9 and at 2^11 (2^4 87 us against 90 / 96 for 4096 / 8192, 2^5
+// 86 against 94 / 131, 2^6 87 against 96 / 133; 2^7 .. 2^9 and 2^11 by one timer tick, ~2 us),
+// the default 4096 at 2^10 and 2^12; 2^13 / 2^14 have one width. -1 = the default.
+static const int kBatchedTunedLogC[kMaxSingleLog2 + 1] = {-1, -1, -1, -1, 7, 6, 5, 4, 3, 2, 2, 0, 0, 0, 0};
+
 static Shape tuned_shape(int m) {
     Shape s{};
     if (m <= kMaxSingleLog2) {
         s.npass = 1;
         s.len[0] = m;
+        s.cols[0] = kBatchedTunedLogC[m];
         return s;
     }
     return kTuned[m - 15];
 }
 
 static bool valid_shape(int m, const Shape &s) {
-    if (s.npass == 1) return s.len[0] == m && m <= kMaxSingleLog2;
+    if (s.npass == 1)
+        return s.len[0] == m && m <= kMaxSingleLog2 && (s.cols[0] == -1 || batched_log_c_supported(m, s.cols[0]));
     if (s.npass < 2 || s.npass > 3) return false;
     int sum = 0;
     for (int p = 0; p < s.npass; ++p) {
@@ -283,6 +293,8 @@ extern "C" onefft_plan *onefft_plan_create_tiles(size_t n, int npass, const int 
         s.len[i] = log2_len[i];
         s.cols[i] = log2_cols ? log2_cols[i] : pass_log_c(log2_len[i]);
     }
+    // one kernel: cols[0] is the transforms per block (log2), the tuned one unless given
+    if (npass == 1 && (!log2_cols || log2_cols[0] == -1)) s.cols[0] = m <= kMaxSingleLog2 ? tuned_shape(m).cols[0] : -1;
     if (!valid_shape(m, s)) {
         set_error(ONEFFT_ERR_ARG, "invalid pass split for n=%zu", n);
         return nullptr;
@@ -363,7 +375,7 @@ static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *
     if (p->npass == 1) {
         g_launches.fetch_add(1);
         if (p->tc) return launch_single_kernel_tc(p->log2n, in, out, batch, p->stw[0], inverse, s);
-        return launch_single_kernel(p->log2n, in, out, batch, p->stw[0], inverse, s, pre, post);
+        return launch_single_kernel(p->log2n, in, out, batch, p->stw[0], inverse, s, pre, post, p->cols[0]);
     }
     PassArgs a{};
     a.log2n = p->log2n;

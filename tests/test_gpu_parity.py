@@ -284,6 +284,35 @@ def test_device_batched_equals_single_bitwise(ofb, oracle, log2n, batch):
     plan.destroy()
 
 
+@pytest.mark.parametrize("log2n", list(range(4, 15)))
+def test_transforms_per_block_same_bits(ofb, oracle, log2n):
+    """Every compiled number of transforms per block of a one-kernel size (the autotuner's
+    choices) gives the default plan's results bit for bit, both directions, with a batch that
+    leaves the last block partly empty; invalid widths are rejected."""
+    from onefft_b200.autotune import batched_log_c_candidates
+    torch = _torch()
+    n = 1 << log2n
+    batch = 2 * (1 << max(0, 13 - log2n)) + 3
+    x = oracle.gen_normal(2 * n * batch, 57 + log2n)
+    d_in = torch.from_numpy(x).cuda()
+    want = torch.empty_like(d_in)
+    default = ofb.Plan(n, split=(log2n,), cols=(max(0, 12 - log2n),))
+    for inv in (False, True):
+        (default.dev_inverse if inv else default.dev_forward)(d_in.data_ptr(), want.data_ptr(), batch)
+        for c in batched_log_c_candidates(log2n):
+            plan = ofb.Plan(n, split=(log2n,), cols=(c,))
+            got = torch.full_like(d_in, float("nan"))
+            (plan.dev_inverse if inv else plan.dev_forward)(d_in.data_ptr(), got.data_ptr(), batch)
+            torch.cuda.synchronize()
+            assert torch.equal(got, want), (log2n, c, inv)
+            plan.destroy()
+    default.destroy()
+    for bad in (max(0, 12 - log2n) + 2, 14 - log2n, -2 if log2n < 12 else 2):
+        if bad not in batched_log_c_candidates(log2n) and bad != -1:
+            with pytest.raises(ValueError):
+                ofb.Plan(n, split=(log2n,), cols=(bad,))
+
+
 def test_device_pointer_contract(ofb):
     torch = _torch()
     L = ofb.lib()
