@@ -128,3 +128,21 @@ def test_python_mirror_raises_on_invalid_size(cuda_lib):
         onefft_b200.forward(np.zeros(6, np.float32))
     with pytest.raises(ValueError):
         onefft_b200.Plan(12)
+
+
+def test_batched_width_rule_matches_autotuner(cuda_lib):
+    """One-pass plans accept exactly the transforms-per-block widths the autotuner times
+    (onefft_b200.autotune.batched_log_c_candidates, plus -1 for the tuned one); any other width
+    is rejected as an invalid split before device work (an accepted width goes on to build the
+    plan, which without a device fails with a CUDA error instead)."""
+    from onefft_b200.autotune import batched_log_c_candidates
+    for log2n in range(4, 15):
+        ok = set(batched_log_c_candidates(log2n)) | {-1}
+        for c in range(-3, 12):
+            lens = (ctypes.c_int * 1)(log2n)
+            cols = (ctypes.c_int * 1)(c)
+            h = cuda_lib.onefft_plan_create_tiles(1 << log2n, 1, lens, cols, 0, 0)
+            rejected = h is None and b"invalid pass split" in cuda_lib.onefft_last_error()
+            if h:
+                cuda_lib.onefft_plan_destroy(h)
+            assert rejected == (c not in ok), (log2n, c)
