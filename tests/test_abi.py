@@ -146,3 +146,18 @@ def test_batched_width_rule_matches_autotuner(cuda_lib):
             if h:
                 cuda_lib.onefft_plan_destroy(h)
             assert rejected == (c not in ok), (log2n, c)
+
+
+def test_autotuner_candidates_are_valid_splits(cuda_lib):
+    """Every multi-pass shape the autotuner times (onefft_b200.autotune.candidates) passes the
+    library's split validation; a shape the library rejects would be timed as an error."""
+    from onefft_b200.autotune import candidates
+    for m in (15, 20, 24, 27, 30):
+        for lens, cols, chunk in candidates(m):
+            k = len(lens)
+            h = cuda_lib.onefft_plan_create_tiles(1 << m, k, (ctypes.c_int * k)(*lens), (ctypes.c_int * k)(*cols),
+                                                  3, chunk)
+            if h:
+                cuda_lib.onefft_plan_destroy(h)
+            else:
+                assert b"invalid pass split" not in cuda_lib.onefft_last_error(), (m, lens, cols, chunk)
