@@ -375,6 +375,8 @@ def main():
         dist.barrier()
     launches = int(L.onefft_debug_launch_count() - launches0)
     clk = clocks.stop()
+    for w in work:  # a kernel failure recorded during the timed steps voids the run
+        w["plan"].check()
     t = events[0][0].elapsed_time(events[-1][-1]) / 1e3
     t = max_over_ranks(t, device="cuda")
     per_step = t / args.steps

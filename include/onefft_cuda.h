@@ -157,8 +157,9 @@ ONEFFT_API int onefft_uneven_execute(onefft_uneven *batch, const float *d_in, fl
  * exits) for the twiddle tables of sizes 2^4 .. 2^16, the sorted descriptors and the work
  * queue. Limits: at most 4096 descriptors per call (more is rejected with -2 and a message in
  * onefft_last_error()), log2n <= 16, same buffer rules as onefft_uneven_execute(). The first
- * call on a device builds the tables there (a few small kernels, then a stream synchronize);
- * make that first call before any stream capture. Later calls only copy the descriptors in,
+ * call on a device builds the tables there (a few small kernels, then a stream synchronize),
+ * and so does the first call after that device's context was reset (cudaDeviceReset); make
+ * such a call before any stream capture. Later calls only copy the descriptors in,
  * zero the queue counter and launch. Every call shares the array and overwrites it: calls
  * whose GPU work overlaps race, so issue them in order (for example on one stream). */
 ONEFFT_API int onefft_uneven_execute_noalloc(const onefft_desc *desc, size_t count, const float *d_in, float *d_out,
@@ -168,6 +169,17 @@ ONEFFT_API int onefft_uneven_execute_noalloc(const onefft_desc *desc, size_t cou
 
 /* Message of the last error in the calling thread ("" if none). */
 ONEFFT_API const char *onefft_last_error(void);
+
+/* Errors that kernels of `plan` found while running, for callers of the device-pointer entry
+ * points (which return as soon as the work is enqueued). The multi-pass kernels wait on their
+ * tile copies with a bounded wait; a wait that runs out makes the kernel record it in the plan's
+ * error word, leave its tile unwritten and return, so the output of that call is not valid.
+ * Returns 0 if no such failure was recorded since the last call, else ONEFFT_ERR_CUDA_BASE with
+ * the reason in onefft_last_error(); reading clears the word. Call it after synchronising the
+ * streams the plan's transforms ran on. The host-pointer calls check the word themselves and
+ * return the error (or leave `out` untouched) instead. Counterpart of OneFFT's error return
+ * (include/onefft.h:73-75) for work that completes after the call returned. */
+ONEFFT_API int onefft_plan_status(const onefft_plan *plan);
 
 /* Test hook: make the k-th device allocation from now on fail (k >= 1), as if the device were
  * out of memory; 0 disarms. Used by the tests of the -1 / untouched-output contract. */
@@ -180,6 +192,13 @@ ONEFFT_API int onefft_debug_twiddles(unsigned log2n, size_t count, float *out);
 
 /* Number of kernel launches this process has issued through the library (all threads). */
 ONEFFT_API unsigned long long onefft_debug_launch_count(void);
+
+/* Test hook of the failure path above: while `on` is non-zero, the first bounded wait of every
+ * tile of the multi-pass kernels on the current device counts as expired, without a real device
+ * failure. Each tile then lets its copy land, records the failure and returns unwritten, so
+ * host-pointer calls return an error with `out` untouched and onefft_plan_status() reports it.
+ * Returns 0, or a CUDA error code. Device state: set it back to 0 before other work. */
+ONEFFT_API int onefft_debug_expire_waits(int on);
 
 #ifdef __cplusplus
 } /* extern "C" */

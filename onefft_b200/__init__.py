@@ -36,7 +36,8 @@ C_SYMBOLS = (
     "onefft_plan_create_split", "onefft_plan_create_tiles", "onefft_plan_create_bf16x3", "onefft_plan_passes",
     "onefft_uneven_create", "onefft_uneven_create_split", "onefft_uneven_destroy", "onefft_uneven_span", "onefft_uneven_execute",
     "onefft_uneven_execute_noalloc",
-    "onefft_last_error", "onefft_debug_fail_alloc", "onefft_debug_twiddles", "onefft_debug_launch_count",
+    "onefft_last_error", "onefft_plan_status", "onefft_debug_fail_alloc", "onefft_debug_twiddles",
+    "onefft_debug_launch_count", "onefft_debug_expire_waits",
 )
 
 _lib: ctypes.CDLL | None = None
@@ -114,6 +115,10 @@ def lib() -> ctypes.CDLL:
     L.onefft_debug_twiddles.restype = ctypes.c_int
     L.onefft_debug_launch_count.argtypes = []
     L.onefft_debug_launch_count.restype = ctypes.c_ulonglong
+    L.onefft_plan_status.argtypes = [_vp]
+    L.onefft_plan_status.restype = ctypes.c_int
+    L.onefft_debug_expire_waits.argtypes = [ctypes.c_int]
+    L.onefft_debug_expire_waits.restype = ctypes.c_int
     _lib = L
     return L
 
@@ -212,6 +217,17 @@ class Plan:
         buf = (ctypes.c_int * 3)()
         k = lib().onefft_plan_passes(self.handle, buf)
         return tuple(buf[i] for i in range(k))
+
+    def status(self) -> int:
+        """onefft_plan_status: 0, or the error code of a kernel failure recorded since the last
+        call (reading clears it); call after synchronising the streams the plan ran on."""
+        return int(lib().onefft_plan_status(self.handle))
+
+    def check(self) -> None:
+        """Raises if a kernel of this plan recorded a failure (see status())."""
+        rc = self.status()
+        if rc != 0:
+            raise RuntimeError(f"transform failed on the device ({rc}): {last_error()}")
 
     def destroy(self) -> None:
         if getattr(self, "_h", None):

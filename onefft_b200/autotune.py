@@ -11,7 +11,7 @@ the fastest shape per size as the C table used by onefft_api.cu (tuned_shape) pl
     python -m onefft_b200.autotune --uneven
 
 tunes the uneven batch instead: the in-block two-pass split of each size 2^13 .. 2^16 among the
-compiled candidates (uneven.cu kSplits), printed as uneven.cu's kUnevenTunedSplit.
+compiled candidates (uneven.h kUnevenSplits), printed as uneven.h's kUnevenTunedSplit.
 
     python -m onefft_b200.autotune --batched
 
@@ -143,7 +143,7 @@ def tune_uneven(reps: int = 9) -> dict:
     """In-block split per size 2^13 .. 2^16 of the uneven batch: for each size, 2^25 / n
     transforms of that size (256 MiB, half of them inverse) executed with every compiled split
     (onefft_uneven_create_split); prints the fastest choice per size as the table
-    kUnevenTunedSplit of uneven.cu. Choice 0 everywhere runs in the kernel compiled with those
+    kUnevenTunedSplit of uneven.h. Choice 0 everywhere runs in the kernel compiled with those
     splits inlined, any other combination in the kernel that calls the split chosen at run time,
     so an alternative must win despite its call overhead; the tuned combination then gets a
     kernel of its own with its splits inlined."""

@@ -173,7 +173,7 @@ struct Stages {
 };
 
 // Stage table length for a runtime tile length (host side sizing).
-__host__ __device__ inline int stage_table_entries(int log_l) {
+__host__ __device__ constexpr int stage_table_entries(int log_l) {
     if (log_l < 4) return 0;
     int n16 = log_l / 4, rem = log_l % 4, count = n16 + (rem ? 1 : 0), o = 0;
     for (int s = 1; s < count; ++s) o += ((1 << (s < n16 ? 4 : rem)) - 1) << (4 * s);

@@ -75,6 +75,9 @@ cudaError_t launch_pass(int mode, int log_l, int log_c, const PassArgs& a, int b
 // TMA-staged passes (fft_tma.cu): same arithmetic as launch_pass; 16-byte aligned buffers,
 // batch <= 65535, shapes pass_tma_supported()
 bool pass_tma_supported(int log_l, int log_c);
+// Test hook: every first bounded wait of the TMA-staged kernels on the current device counts as
+// expired while `on` (onefft_debug_expire_waits).
+cudaError_t set_expire_waits(int on);
 cudaError_t launch_pass_tma(int mode, int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t stream);
 // split-BF16 tensor-core variants (fft_tc.cu): n = 2^4 .. 2^14 in one kernel; pass lengths
 // 2^5 .. 2^12 with the default tile width pass_log_c()
@@ -89,6 +92,9 @@ cudaError_t launch_big_table(double2* lo, double2* hi, int log2n, int lo_bits, c
 int stage_table_entries_host(int log_l);
 // Sets the calling thread's onefft_last_error() message.
 void record_error(const char *msg);
+// Kernel launches issued through the library (onefft_debug_launch_count); every entry point that
+// launches a kernel adds to it.
+extern std::atomic<unsigned long long> g_launches;
 cudaError_t launch_twiddle_probe(float2* dst, unsigned log2n, unsigned long long count, cudaStream_t stream);
 
 }  // namespace ofb

@@ -23,6 +23,17 @@ namespace ofb {
 
 constexpr unsigned kWaitLimit = 1u << 22;  // try_wait polls (each may suspend briefly): ~0.1-1 s
 
+// Test hook of the failure path (onefft_debug_expire_waits): when non-zero, the first wait of
+// every tile counts as expired without polling. The tile then takes the same path as after a
+// real expiry: it records the failure in the plan's error word, lets its copy land (the normal
+// bounded wait) and returns without writing.
+__device__ int g_expire_waits = 0;
+
+cudaError_t set_expire_waits(int on) {
+    const int v = on ? 1 : 0;
+    return cudaMemcpyToSymbol(g_expire_waits, &v, sizeof v);
+}
+
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
@@ -177,7 +188,7 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_
         wjf = pass_twiddle_lane<LOG_L>(a, MODE == 0 ? col0 + c : (col0 >> a.log_s) << a.log_s, j);
     }
     __syncthreads();  // the barrier is initialised before anyone waits on it
-    const bool ok = mbar_wait(bar, 0);
+    const bool ok = !g_expire_waits && mbar_wait(bar, 0);
     if (__syncthreads_or(!ok)) {
         if (tid == 0) {
             *(volatile unsigned*)a.err = 1u;

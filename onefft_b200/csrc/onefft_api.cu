@@ -36,7 +36,7 @@ using namespace ofb;
 
 static thread_local std::string t_last_error;
 static std::atomic<int> g_fail_alloc_countdown{0};
-std::atomic<unsigned long long> g_launches{0};
+std::atomic<unsigned long long> ofb::g_launches{0};
 
 static int set_error(int code, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
 static int set_error(int code, const char *fmt, ...) {
@@ -645,10 +645,10 @@ struct DeviceGuard {
 
 }  // namespace
 
-// After a synchronise: 0, or an error if a TMA kernel of the plan recorded an expired wait in
-// the plan's error word (which is then cleared).
+// After a synchronise: 0, or an error if a kernel of the plan recorded an expired bounded wait
+// in the plan's error word (which is then cleared).
 static int kernel_error(const onefft_plan *p) {
-    if (!p->tma) return 0;
+    if (!p->err_host) return 0;
     volatile unsigned *word = p->err_host;
     const unsigned flag = *word;
     if (!flag) return 0;
@@ -723,6 +723,18 @@ static int host_execute(const onefft_plan *p, const float *in, float *out, size_
     if (e == cudaSuccess) e = e2;
     if (e != cudaSuccess) return cuda_error(e, "transform");
     return kernel_error(p);
+}
+
+extern "C" int onefft_plan_status(const onefft_plan *plan) {
+    t_last_error.clear();
+    if (!plan) return set_error(ONEFFT_ERR_ARG, "NULL plan");
+    return kernel_error(plan);
+}
+
+extern "C" int onefft_debug_expire_waits(int on) {
+    t_last_error.clear();
+    const cudaError_t e = set_expire_waits(on);
+    return e == cudaSuccess ? 0 : cuda_error(e, "wait-expiry hook");
 }
 
 extern "C" void onefft_plan_forward(const onefft_plan *plan, const float *in, float *out) {

@@ -33,26 +33,9 @@
 
 namespace ofb {
 
-// Two-pass splits (L0, L1) of the sizes handled by one block, kUnevenSplitChoices per log2 n.
-// Choice 0 is the plain path's split where it has one (2^15, 2^16), so that the batch reproduces
-// the plain path bit for bit; the others are the candidates that onefft_b200/autotune.py times.
-constexpr int kSplits[4][kUnevenSplitChoices][2] = {
-    {{7, 6}, {6, 7}, {8, 5}},  // 2^13
-    {{7, 7}, {8, 6}, {6, 8}},  // 2^14
-    {{8, 7}, {7, 8}, {9, 6}},  // 2^15
-    {{8, 8}, {9, 7}, {7, 9}},  // 2^16
-};
-
-// The split the batch uses per size 2^13 .. 2^16 unless told otherwise, measured by
-// `python -m onefft_b200.autotune --uneven` on a B200 (2^25 values of one size per batch, half of
-// them inverse): 2^13 (7,6) 183 us, (6,7) 216 us, (8,5) 158 us; 2^14 (7,7) 207 us, (8,6) 183 us,
-// (6,8) 227 us; 2^15 (8,7) 206 us, (7,8) 221 us, (9,6) 239 us; 2^16 (8,8) 234 us, (9,7) 277 us,
-// (7,9) 299 us.
-constexpr int kUnevenTunedSplit[4] = {2, 1, 0, 0};
-
 int uneven_split(int m, int choice, int pass) {
     if (m < 13 || m > 16 || choice < 0 || choice >= kUnevenSplitChoices) return 0;
-    return kSplits[m - 13][choice][pass ? 1 : 0];
+    return kUnevenSplits[m - 13][choice][pass ? 1 : 0];
 }
 
 // Tile width of an in-block pass of length 2^L: 16 columns, fewer when the tile would exceed
@@ -144,13 +127,13 @@ __device__ __forceinline__ void big_choice(const UnevenArgs& a, const onefft_des
     const BigItemArgs b{a.in + d.offset, a.out + d.offset, a.tw_lo[M], a.tw_hi[M],
                         a.stw[M][0],     a.stw[M][1],      a.lo_bits[M], d.inverse};
     if constexpr (CHOICE != kSplitAtRunTime) {
-        big_item<M, kSplits[I][CHOICE][0], kSplits[I][CHOICE][1]>(b, smem, tid);
+        big_item<M, kUnevenSplits[I][CHOICE][0], kUnevenSplits[I][CHOICE][1]>(b, smem, tid);
     } else {
         static_assert(kUnevenSplitChoices == 3, "one branch per compiled split");
         switch (a.split[M]) {
-        case 1: big_item_call<M, kSplits[I][1][0], kSplits[I][1][1]>(b, smem, tid); break;
-        case 2: big_item_call<M, kSplits[I][2][0], kSplits[I][2][1]>(b, smem, tid); break;
-        default: big_item_call<M, kSplits[I][0][0], kSplits[I][0][1]>(b, smem, tid); break;
+        case 1: big_item_call<M, kUnevenSplits[I][1][0], kUnevenSplits[I][1][1]>(b, smem, tid); break;
+        case 2: big_item_call<M, kUnevenSplits[I][2][0], kUnevenSplits[I][2][1]>(b, smem, tid); break;
+        default: big_item_call<M, kUnevenSplits[I][0][0], kUnevenSplits[I][0][1]>(b, smem, tid); break;
         }
     }
 }
@@ -176,7 +159,7 @@ __device__ __forceinline__ void tiny_item(const UnevenArgs& a, const UnevenItem&
 // 20000 transforms of 2^4 .. 2^16, 1.21 ms at 2 blocks per SM (128 registers), 1.14 ms at 3
 // (80 registers), 1.12 ms at 4; items are latency-bound tile sequences, so more resident blocks
 // hide more of each block's waits.
-// C13 .. C16: the split of each size 2^13 .. 2^16 (an index into kSplits, or kSplitAtRunTime).
+// C13 .. C16: the split of each size 2^13 .. 2^16 (an index into kUnevenSplits, or kSplitAtRunTime).
 template <int C13, int C14, int C15, int C16>
 __global__ void __launch_bounds__(kUnevenThreads, 4) k_uneven(UnevenArgs a) {
     extern __shared__ float2 smem[];

@@ -11,6 +11,28 @@ namespace ofb {
 constexpr int kUnevenMaxLog2 = 16;
 constexpr int kUnevenSplitChoices = 3;  // compiled two-pass splits per size 2^13 .. 2^16
 
+// Two-pass splits (L0, L1) of the sizes one block handles, kUnevenSplitChoices per log2 n.
+// Choice 0 is the plain path's split where it has one (2^15, 2^16), so that the batch reproduces
+// the plain path bit for bit; the others are the candidates that onefft_b200/autotune.py times.
+constexpr int kUnevenSplits[4][kUnevenSplitChoices][2] = {
+    {{7, 6}, {6, 7}, {8, 5}},  // 2^13
+    {{7, 7}, {8, 6}, {6, 8}},  // 2^14
+    {{8, 7}, {7, 8}, {9, 6}},  // 2^15
+    {{8, 8}, {9, 7}, {7, 9}},  // 2^16
+};
+
+// The split the batch uses per size 2^13 .. 2^16 unless told otherwise, measured by
+// `python -m onefft_b200.autotune --uneven` on a B200 (2^25 values of one size per batch, half of
+// them inverse): 2^13 (7,6) 183 us, (6,7) 216 us, (8,5) 158 us; 2^14 (7,7) 207 us, (8,6) 183 us,
+// (6,8) 227 us; 2^15 (8,7) 206 us, (7,8) 221 us, (9,6) 239 us; 2^16 (8,8) 234 us, (9,7) 277 us,
+// (7,9) 299 us.
+constexpr int kUnevenTunedSplit[4] = {2, 1, 0, 0};
+
+// Pass length (log2) of pass `pass` of the tuned split of 2^m, 13 <= m <= 16.
+constexpr int uneven_tuned_len(int m, int pass) {
+    return kUnevenSplits[m - 13][kUnevenTunedSplit[m - 13]][pass ? 1 : 0];
+}
+
 // One work item: `count` transforms of size 2^log2n at desc[first .. first + count).
 struct UnevenItem {
     int log2n;

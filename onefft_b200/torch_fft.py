@@ -12,7 +12,9 @@ the inverse is the forward transform.
 ``weighted_power_loss(x, w)`` is the loss of the differentiable-layer benchmark configuration,
 sum |w * fft(x)|^2, built from these pieces; its gradient is 2 F^H (w^2 * F x).
 
-No CPU path exists: CPU tensors raise.
+No CPU path exists: CPU tensors raise. The transforms only enqueue work; a failure that a
+multi-pass kernel finds while running (an expired bounded wait) is reported by ``check()`` after
+the caller synchronises.
 """
 from __future__ import annotations
 
@@ -37,6 +39,15 @@ def _plan(n: int, device: int) -> Plan:
                     p = Plan(n)
                 _plans[key] = p
     return p
+
+
+def check() -> None:
+    """Raises if a kernel of any plan this module used recorded a failure since the last check
+    (onefft_plan_status); call after synchronising the streams the transforms ran on."""
+    with _plans_lock:
+        plans = list(_plans.values())
+    for p in plans:
+        p.check()
 
 
 def _check(x: torch.Tensor) -> torch.Tensor:

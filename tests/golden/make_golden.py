@@ -12,7 +12,7 @@ of the test suite and stores
   ref_errors.json   the reference's relative RMS (tests/test_onefft.c:64-71) and max-abs error
                     against the FP64 oracle, per size and direction, on the suite's inputs for
                     every size of the configurations (uniform per size up to 2^20; standard
-                    normal at 4096, 2^16, 2^20, 2^22, 2^24; the n=1024 config-1 input).
+                    normal at 2^10, 2^12, 2^13, 2^16, 2^20, 2^22 and 2^24 .. 2^27).
 
 Usage:  python tests/golden/make_golden.py   (needs the reference tree; run where it exists)
 """
@@ -70,7 +70,7 @@ def main() -> None:
             small[f"in_{l}"] = x
         errors["uniform"][str(l)] = rec
         print(l, rec["forward"]["rel_rms"], rec["inverse"]["rel_rms"], flush=True)
-    for l in (10, 12, 13, 16, 20, 22, 24):
+    for l in (10, 12, 13, 16, 20, 22, 24, 25, 26, 27):
         x = O.gen_normal(2 * (1 << l), SEED_NORMAL + l)
         rec = {}
         for inv in (0, 1):

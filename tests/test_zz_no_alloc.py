@@ -7,11 +7,12 @@ persistent kernel as onefft_uneven_execute, with its twiddle tables, descriptors
 in one fixed device array instead of a batch object's allocation.
 
 The test checks two calls in a row, each with a different descriptor list, against the existing
-entry point (onefft_uneven_create + onefft_uneven_execute) on the same inputs: every transform
-within the reference's error bound of the existing result (they run the same kernel and tables,
-so the results are in fact identical), and that the array left behind by the first call does
-not leak into the second. It also checks the stated limit. The file is named to be collected
-last, and it needs nothing from the other test files.
+entry point (onefft_uneven_create + onefft_uneven_execute) on the same inputs. Both run the same
+kernel (the tuned in-block splits) with tables built by the same kernels, so every transform
+must equal the existing result bit for bit (and so lie within the reference's error bound of
+it); the second call also shows that the array left behind by the first does not leak into it.
+It also checks the stated limit. The file is named to be collected last, and it needs nothing
+from the other test files.
 """
 from __future__ import annotations
 
@@ -58,13 +59,12 @@ def test_noalloc_matches_existing_entry_point_on_two_calls(ofb, oracle):
         T.cuda.synchronize()
         existing.destroy()
         g, w = got.cpu().numpy(), want.cpu().numpy()
-        same = 0
         for m, off in zip(desc["log2n"].tolist(), desc["offset"].tolist()):
             n = 1 << m
             a, b = g[2 * off:2 * (off + n)], w[2 * off:2 * (off + n)]
             assert oracle.rel_rms(a, b.astype(np.float64)) <= oracle.tolerance(m), (seed, m, off)
-            same += int(np.array_equal(a.view(np.uint32), b.view(np.uint32)))
-        print(f"no-alloc call with {count} transforms: {same} of {count} identical to the existing entry point")
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (seed, m, off)
+        print(f"no-alloc call with {count} transforms: all identical to the existing entry point")
 
 
 def test_noalloc_rejects_more_than_the_limit(ofb):
