@@ -190,9 +190,9 @@ def run_reference(args, rank: int):
     """--impl reference: the reference CPU library on this host, rank 0 only."""
     if rank != 0:
         return
-    # a step is ~1-1.5 s of host work: at most 5 timed and 3 warm-up steps keep the run short
-    steps = max(1, min(args.steps, 5))
-    warmup = max(1, min(args.warmup, 3))
+    # a step is ~1-1.5 s of host work: the requested 20 + 5 steps take about half a minute
+    steps = max(1, args.steps)
+    warmup = max(1, args.warmup)
     times, cores, kind, impl = cpu_step_times(steps, warmup)
     t = sum(times) / len(times)
     value = STEP_FLOPS / t / 1e9
@@ -224,11 +224,74 @@ def _time(torch, stream, fn, reps: int = 5, warm: int = 2) -> float:
     return e0.elapsed_time(e1) / 1e3 / reps
 
 
-def other_configs(torch, ofb, L, stream, peak):
-    """The uneven batch, the split-BF16 variant and the differentiable layer, each against the
-    plain FP32 GPU path on the same data (accuracy of each is checked by the test suite)."""
+def config1_latency(torch, ofb, L, stream):
+    """One n = 1024 forward + inverse (the latency-bound configuration), as the reference's
+    bench/bench.c:151-167 times it: the minimum over samples of one call pair, through the
+    drop-in host API on pageable and on pinned host buffers (copies, launch and synchronisation
+    included), and through the device-pointer entry points with a stream synchronisation; the
+    reference library on one host core beside it."""
+    n, log2n = 1024, 10
+    pair_flops = 2 * 5.0 * n * log2n
+    rng = np.random.default_rng(0xC0F1)
+    xh = rng.uniform(-1, 1, 2 * n).astype(np.float32)
+    yh, zh = np.empty_like(xh), np.empty_like(xh)
+    xp = torch.from_numpy(xh).pin_memory()
+    yp, zp = torch.empty_like(xp).pin_memory(), torch.empty_like(xp).pin_memory()
+    plan = ofb.Plan(n)
+    xd = xp.cuda()
+    yd, zd = torch.empty_like(xd), torch.empty_like(xd)
     sptr = stream.cuda_stream
-    out = {}
+
+    def sample(fn, reps=400, warm=50):
+        for _ in range(warm):
+            fn()
+        best = float("inf")
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            fn()
+            best = min(best, time.perf_counter() - t0)
+        return best
+
+    def host_pageable():
+        L.onefft_forward(xh.ctypes.data, yh.ctypes.data, n)
+        L.onefft_inverse(yh.ctypes.data, zh.ctypes.data, n)
+
+    def host_pinned():
+        L.onefft_forward(xp.data_ptr(), yp.data_ptr(), n)
+        L.onefft_inverse(yp.data_ptr(), zp.data_ptr(), n)
+
+    def device():
+        plan.dev_forward(xd.data_ptr(), yd.data_ptr(), 1, sptr)
+        plan.dev_inverse(yd.data_ptr(), zd.data_ptr(), 1, sptr)
+        stream.synchronize()
+
+    t_pg, t_pn, t_d = sample(host_pageable), sample(host_pinned), sample(device)
+    ok = bool(np.allclose(zh, xh * n, rtol=0, atol=1e-3 * n))
+    res = {"us_host_api_pageable": 1e6 * t_pg, "us_host_api_pinned": 1e6 * t_pn, "us_device_pointers": 1e6 * t_d,
+           "gflops_host_api_pinned": pair_flops / t_pn / 1e9, "round_trip_ok": ok,
+           "note": "min over 400 samples of one forward + inverse pair (wall clock, synchronous)"}
+    try:
+        import oracle
+        if oracle.have_reference():
+            batch = 4096
+            xb = np.tile(xh, batch)
+            ob = np.empty_like(xb)
+            t_f = oracle.cpu_bench_batched(n, batch, 1, False, xb, ob, 5) / batch
+            t_i = oracle.cpu_bench_batched(n, batch, 1, True, xb, ob, 5) / batch
+            res["us_reference_cpu_1thread"] = 1e6 * (t_f + t_i)
+            res["reference_impl"] = oracle.cpu_impl()
+    except Exception as e:  # reported, not fatal
+        res["reference_error"] = str(e)
+    plan.destroy()
+    return res
+
+
+def other_configs(torch, ofb, L, stream, peak):
+    """The latency-bound n = 1024 pair, the uneven batch, the split-BF16 variant and the
+    differentiable layer, each against the plain FP32 GPU path on the same data (accuracy of each
+    is checked by the test suite)."""
+    sptr = stream.cuda_stream
+    out = {"config1 n=1024 fwd+inv latency": config1_latency(torch, ofb, L, stream)}
     g = torch.Generator(device="cuda").manual_seed(99)
     # uneven batch: 20000 transforms, log2 n uniform in 4..16, packed, half inverse
     rng = np.random.default_rng(0xC0F3)
@@ -239,6 +302,8 @@ def other_configs(torch, ofb, L, stream, peak):
     x = torch.rand(2 * ub.span, device="cuda", generator=g) * 2 - 1
     y = torch.empty_like(x)
     t_u = _time(torch, stream, lambda: ub.execute(x.data_ptr(), y.data_ptr(), sptr))
+    if ub.status() != 0:
+        raise RuntimeError(f"uneven batch failed on the device: {ofb.last_error()}")
     plans = {m: ofb.Plan(1 << m) for m in range(4, 17)}
     base_in, base_out = x.data_ptr(), y.data_ptr()
     calls = [((L.onefft_dev_inverse_batched if i else L.onefft_dev_forward_batched), plans[m].handle,
@@ -249,14 +314,34 @@ def other_configs(torch, ofb, L, stream, peak):
             f(h, a, b, 1, sptr)
 
     t_p = _time(torch, stream, per_transform, reps=2, warm=1)
+    # the plain path at its best: the same transforms already grouped by size and direction into
+    # contiguous batches (the grouping copy is not timed), one batched call per group
+    groups = []
+    for m in range(4, 17):
+        for d in (0, 1):
+            sel = np.nonzero((log2n == m) & (inv == d))[0]
+            if sel.size == 0:
+                continue
+            idx = torch.from_numpy((off[sel][:, None] + np.arange(1 << m)[None, :]).reshape(-1)).cuda()
+            gx = torch.view_as_real(torch.view_as_complex(x.view(-1, 2))[idx]).reshape(-1).contiguous()
+            groups.append((plans[m], d, int(sel.size), gx, torch.empty_like(gx)))
+
+    def grouped():
+        for p, d, cnt, gx, gy in groups:
+            (p.dev_inverse if d else p.dev_forward)(gx.data_ptr(), gy.data_ptr(), cnt, sptr)
+
+    t_g = _time(torch, stream, grouped)
     flops = float(sum(5.0 * (1 << m) * m for m in log2n.tolist()))
     out["uneven 20000 x 2^(4..16)"] = {
-        "us_persistent": 1e6 * t_u, "us_per_transform_calls": 1e6 * t_p, "speedup": t_p / t_u,
+        "us_persistent": 1e6 * t_u, "us_plain_grouped": 1e6 * t_g, "us_per_transform_calls": 1e6 * t_p,
+        "speedup_vs_grouped": t_g / t_u, "speedup_vs_per_transform": t_p / t_u,
         "gflops": flops / t_u / 1e9, "gbs_16n": 16 * ub.span / t_u / 1e9, "frac_hbm": 16 * ub.span / t_u / 1e9 / peak,
-        "note": "one persistent launch vs one onefft_dev_*_batched call per transform (plain FP32 path); "
-                "results equal bit for bit except 2^13/2^14 (tests/test_gpu_uneven.py)"}
+        "note": "one persistent launch vs (a) the plain FP32 path on the same transforms grouped by size and "
+                "direction into contiguous batches, one onefft_dev_*_batched call per group (grouping copy not "
+                "timed), and (b) one onefft_dev_*_batched call per transform; results equal the plain path bit "
+                "for bit except 2^13/2^14 (tests/test_gpu_uneven.py)"}
     ub.destroy()
-    del x, y
+    del x, y, groups
     # split-BF16 tensor-core variant vs plain FP32 on the same batches
     for lg, batch in ((16, 256), (22, 16)):
         n = 1 << lg

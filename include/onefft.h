@@ -84,7 +84,9 @@ ONEFFT_API const char *onefft_implementation(void);
 
 #include <complex>
 
-/* C++ convenience layer with the same shape as OneFFT's (include/onefft.h:123-169). */
+/* C++ convenience layer: OneFFT's own (include/onefft.h:123-169), kept with the same names,
+ * signatures and behaviour so C++ callers compile unchanged; get() is added.
+ * OneFFT's C++ layer: Copyright (c) 2026 Torben Thaysen, MIT License. */
 namespace onefft {
 
 inline bool forward(const std::complex<float> *in, std::complex<float> *out, std::size_t n) {

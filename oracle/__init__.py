@@ -34,12 +34,18 @@ _i64p = ctypes.POINTER(ctypes.c_int64)
 _sz = ctypes.c_size_t
 
 
+# Where the OneFFT tree is mounted on the machine that builds the checker (read-only; the GPU
+# machines have no copy and use the prebuilt oracle/_ref/). ONEFFT_REFERENCE_DIR overrides it.
+REFERENCE_DIR = os.environ.get("ONEFFT_REFERENCE_DIR", "/root/reference")
+
+
 def build(reference_dir: str | None = None) -> None:
-    """Compile liboracle.so and, when the reference sources exist, oracle/_ref/."""
+    """Compile liboracle.so and, when the reference sources exist, oracle/_ref/ from them."""
     env = dict(os.environ)
     args = ["make", "-C", HERE, "--no-print-directory"]
-    if reference_dir:
-        args.append(f"REF={reference_dir}")
+    ref = reference_dir or REFERENCE_DIR
+    if ref and os.path.exists(os.path.join(ref, "src", "onefft.c")):
+        args.append(f"REF={ref}")
     subprocess.run(args, check=True, env=env, stdout=subprocess.DEVNULL)
 
 

@@ -1,6 +1,8 @@
-"""The drop-in API from C: tests/c_api/check_c_api.c is compiled as C99 against include/onefft.h
-and linked to libonefft_cuda.so the way a OneFFT caller would link (cc ... -lonefft_cuda).
-Compiling and linking needs no GPU; running the program's checks does.
+"""The drop-in API from C and C++: tests/c_api/check_c_api.c is compiled as C99 and
+tests/c_api/check_cpp_api.cpp as C++11 (the C++ layer of the header, as OneFFT's
+tests/test_cpp.cpp uses it) against include/onefft.h, each linked to libonefft_cuda.so the way a
+OneFFT caller would link (cc / c++ ... -lonefft_cuda). Compiling and linking needs no GPU;
+running the programs' checks does.
 """
 from __future__ import annotations
 
@@ -12,23 +14,32 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SRC = os.path.join(ROOT, "tests", "c_api", "check_c_api.c")
+SRC_CPP = os.path.join(ROOT, "tests", "c_api", "check_cpp_api.cpp")
 
 
-def build_c_program(out_dir: str) -> str:
+def _build(out_dir: str, src: str, compilers: tuple[str, ...], std: str, name: str) -> str:
     import onefft_b200
     if not os.path.exists(onefft_b200.LIB_PATH):
         from onefft_b200 import build
         build.build()
-    cc = shutil.which("cc") or shutil.which("gcc")
+    cc = next((c for c in map(shutil.which, compilers) if c), None)
     if cc is None:
-        pytest.skip("no C compiler")
-    exe = os.path.join(out_dir, "check_c_api")
+        pytest.skip(f"no compiler among {compilers}")
+    exe = os.path.join(out_dir, name)
     libdir = os.path.dirname(onefft_b200.LIB_PATH)
-    cmd = [cc, "-std=c99", "-O2", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"), SRC,
+    cmd = [cc, f"-std={std}", "-O2", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"), src,
            "-L", libdir, "-lonefft_cuda", f"-Wl,-rpath,{libdir}", "-lm", "-o", exe]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     return exe
+
+
+def build_c_program(out_dir: str) -> str:
+    return _build(out_dir, SRC, ("cc", "gcc"), "c99", "check_c_api")
+
+
+def build_cpp_program(out_dir: str) -> str:
+    return _build(out_dir, SRC_CPP, ("c++", "g++"), "c++11", "check_cpp_api")
 
 
 def test_c_program_compiles_and_links(tmp_path):
@@ -40,6 +51,21 @@ def test_c_program_compiles_and_links(tmp_path):
 @pytest.mark.gpu
 def test_c_program_checks_pass(tmp_path):
     exe = build_c_program(str(tmp_path))
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "all checks passed" in r.stdout
+
+
+def test_cpp_program_compiles_and_links(tmp_path):
+    """The header's C++ layer compiles as C++11 and links against the library."""
+    exe = build_cpp_program(str(tmp_path))
+    assert os.path.exists(exe)
+
+
+@pytest.mark.gpu
+def test_cpp_program_checks_pass(tmp_path):
+    exe = build_cpp_program(str(tmp_path))
     r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
