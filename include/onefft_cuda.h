@@ -98,6 +98,13 @@ ONEFFT_API onefft_plan *onefft_plan_create_split(size_t n, int npass, const int 
  * each chunk's intermediate values stay in L2 (0 = whole passes). */
 #define ONEFFT_OPT_L2_KEEP 1
 #define ONEFFT_OPT_TMA 2
+/* ONEFFT_OPT_FUSED (three passes, log2_chunk > 0, with ONEFFT_OPT_TMA): the first two passes run
+ * as ONE persistent kernel that takes their tiles chunk by chunk, pass 1 of a chunk as soon as
+ * pass 0 of it is done, so the values between them are re-read from L2 rather than HBM; pass 1
+ * trails pass 0 by ONEFFT_OPT_LAG(k) chunks (1 .. 15; default 1). Results equal the separate
+ * passes bit for bit. */
+#define ONEFFT_OPT_FUSED 4
+#define ONEFFT_OPT_LAG(k) ((k) << 8)
 ONEFFT_API onefft_plan *onefft_plan_create_tiles(size_t n, int npass, const int *log2_len, const int *log2_cols,
                                                  int options, int log2_chunk);
 

@@ -184,9 +184,11 @@ class Plan:
 
     def __init__(self, n: int, split: tuple[int, ...] | None = None, cols: tuple[int, ...] | None = None,
                  l2_keep: bool = True, chunk: int = 0, bf16x3: bool = False, require_accepted: bool = False,
-                 tma: bool = False):
+                 tma: bool = False, fuse_lag: int = 0):
         """split: log2 pass lengths (None = tuned table); cols: log2 tile widths per pass;
         chunk: three passes only, log2 last-digit columns per L2-resident chunk (0 = none);
+        fuse_lag: with chunk and tma, run passes 0 and 1 as one persistent kernel with pass 1
+        trailing pass 0 by this many chunks (ONEFFT_OPT_FUSED; 0 = separate launches);
         bf16x3: the split-BF16 tensor-core variant (require_accepted: only at sizes where it
         meets the FP32 error bound)."""
         L = lib()
@@ -197,7 +199,8 @@ class Plan:
         else:
             arr = (ctypes.c_int * len(split))(*split)
             carr = (ctypes.c_int * len(split))(*cols) if cols is not None else None
-            options = (1 if l2_keep else 0) | (2 if tma else 0)  # ONEFFT_OPT_L2_KEEP | ONEFFT_OPT_TMA
+            # ONEFFT_OPT_L2_KEEP | ONEFFT_OPT_TMA | ONEFFT_OPT_FUSED | ONEFFT_OPT_LAG(fuse_lag)
+            options = (1 if l2_keep else 0) | (2 if tma else 0) | ((4 | (fuse_lag << 8)) if fuse_lag else 0)
             h = L.onefft_plan_create_tiles(n, len(split), arr, carr, options, int(chunk))
         if not h:
             raise ValueError(f"no plan for n={n}: {last_error()}")

@@ -17,6 +17,15 @@ compiled candidates (uneven.h kUnevenSplits), printed as uneven.h's kUnevenTuned
 
 tunes the one-kernel sizes 2^4 .. 2^14: whole transforms per thread block (the default 4096 / n,
 half or twice that), printed as onefft_api.cu's kBatchedTunedLogC.
+
+    python -m onefft_b200.autotune --fused [--min 22] [--max 30]
+
+times, for the three-pass sizes, the first two passes fused into one persistent kernel
+(fft_tma.cu k_pass01_fused): every compiled tile pair, chunk size of the last digit and lag of
+pass 1 behind pass 0, with and without the L2 hints, against the current table's shape; each
+result must equal the separate passes bit for bit. The L2 is flushed before each repetition by
+reading a 512 MiB buffer (clean lines, so no write-backs land in the timed region). Prints the
+table rows with the fuse_lag field.
 """
 from __future__ import annotations
 
@@ -64,6 +73,96 @@ def candidates(m: int):
                     if cs[0] <= g < ls[2]:
                         out.append((ls, cs, g))
     return out
+
+
+# Tile pairs (L0, C0, L1, C1) of the fused passes 0+1 (fft_tma.cu, pass01_fused_supported).
+FUSED_PAIRS = {(8, 4, 9, 3), (8, 3, 8, 3), (8, 4, 8, 4), (8, 3, 7, 4), (9, 3, 9, 3), (10, 3, 10, 3),
+               (10, 3, 11, 2)}
+
+
+def fused_candidates(m: int):
+    """(lengths, widths, chunk bits, lag) of fused three-pass shapes for 2^m."""
+    out = []
+    for l0, c0, l1, c1 in sorted(FUSED_PAIRS):
+        l2 = m - l0 - l1
+        if not 4 <= l2 <= 12:
+            continue
+        for c2 in (2, 3, 4):
+            if not tile_ok(l2, c2) or l2 + c2 < 11 or c0 > l2:
+                continue
+            for g in range(c0, l2 + 1):
+                chunks = 1 << (l2 - g)
+                for lag in (1, 2, 3):
+                    if lag <= chunks:
+                        out.append(((l0, l1, l2), (c0, c1, c2), g, lag))
+    return out
+
+
+def tune_fused(lo: int, hi: int, reps: int) -> dict:
+    flush = torch.ones(1 << 27, dtype=torch.float32, device="cuda")  # read to evict the L2
+
+    def timed(plan, x, y):
+        stream = torch.cuda.current_stream()
+        ts = []
+        for r in range(reps + 2):
+            flush.max()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            plan.dev_forward(x.data_ptr(), y.data_ptr(), 1, stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if r >= 2:
+                ts.append(e0.elapsed_time(e1) * 1e3)
+        ts.sort()
+        return ts[len(ts) // 2]
+
+    results = {}
+    for m in range(lo, hi + 1):
+        n = 1 << m
+        x = torch.randn(2 * n, device="cuda")
+        y = torch.empty_like(x)
+        ref = torch.empty_like(x)
+        base = ofb.Plan(n)
+        base_us = timed(base, x, y)
+        rows = []
+        separate = {}
+        for ls, cs, g, lag in fused_candidates(m):
+            if (ls, cs) not in separate:
+                p = ofb.Plan(n, split=ls, cols=cs, tma=True)
+                p.dev_forward(x.data_ptr(), ref.data_ptr(), 1)
+                torch.cuda.synchronize()
+                separate[(ls, cs)] = ref.clone()
+                p.destroy()
+            for keep in (False, True):
+                try:
+                    p = ofb.Plan(n, split=ls, cols=cs, chunk=g, tma=True, fuse_lag=lag, l2_keep=keep)
+                except ValueError:
+                    continue
+                y.fill_(float("nan"))
+                p.dev_forward(x.data_ptr(), y.data_ptr(), 1)
+                torch.cuda.synchronize()
+                if p.status() != 0 or not torch.equal(y, separate[(ls, cs)]):
+                    raise RuntimeError(f"2^{m} {ls} {cs} chunk {g} lag {lag}: fused result differs")
+                us = timed(p, x, y)
+                p.destroy()
+                rows.append({"len": ls, "cols": cs, "chunk": g, "lag": lag, "l2_keep": keep, "us": us})
+        rows.sort(key=lambda r: r["us"])
+        best = rows[0] if rows else None
+        results[m] = {"base_us": base_us, "best": best, "top": rows[:8]}
+        if best:
+            print(f"m={m}: fused best {best['len']} cols {best['cols']} chunk {best['chunk']} lag {best['lag']} "
+                  f"keep={best['l2_keep']} {best['us']:.1f} us; current table {base_us:.1f} us", flush=True)
+        base.destroy()
+        del x, y, ref, separate
+        torch.cuda.empty_cache()
+    print("// fused shapes: {npass, {len}, {cols}, l2_keep, chunk, tma, fuse_lag}")
+    for m, r in results.items():
+        b = r["best"]
+        if b and b["us"] < r["base_us"]:
+            ls, cs = b["len"], b["cols"]
+            print(f"    /* {m} */ {{3, {{{ls[0]}, {ls[1]}, {ls[2]}}}, {{{cs[0]}, {cs[1]}, {cs[2]}}}, "
+                  f"{int(b['l2_keep'])}, {b['chunk']}, 1, {b['lag']}}},  // {b['us']:.1f} us (was {r['base_us']:.1f})")
+    return results
 
 
 def time_plan(plan, x, y, reps: int, flush) -> float:
@@ -197,7 +296,14 @@ def main():
     ap.add_argument("--chunked-only", action="store_true", help="only TMA-staged variants with L2-resident chunks")
     ap.add_argument("--uneven", action="store_true", help="tune the uneven batch's in-block splits instead")
     ap.add_argument("--batched", action="store_true", help="tune the transforms per block of sizes 2^4 .. 2^14")
+    ap.add_argument("--fused", action="store_true", help="tune the fused first two passes of three-pass sizes")
     args = ap.parse_args()
+    if args.fused:
+        res = tune_fused(max(args.min, 22), args.max, args.reps)
+        if args.out:
+            with open(args.out, "w") as f:
+                json.dump(res, f, indent=1)
+        return
     if args.uneven or args.batched:
         res = tune_uneven() if args.uneven else tune_batched()
         if args.out:

@@ -78,6 +78,14 @@ bool pass_tma_supported(int log_l, int log_c);
 // Test hook: every first bounded wait of the TMA-staged kernels on the current device counts as
 // expired while `on` (onefft_debug_expire_waits).
 cudaError_t set_expire_waits(int on);
+// Passes 0 and 1 of a three-pass transform (pass lengths 2^l0, 2^l1, 2^len2, tile widths 2^c0,
+// 2^c1) in ONE persistent launch over chunks of 2^g last-digit columns, pass 1 trailing pass 0 by
+// `lag` chunks (fft_tma.cu, k_pass01_fused). a0 / a1: the arguments of the chunked launches of
+// passes 0 and 1 (ntiles = tiles per chunk; the per-chunk bases are ignored); one transform.
+// ctr: 2 + 2^(len2 - g) zeroed words used by no concurrent launch (zero again afterwards).
+bool pass01_fused_supported(int l0, int c0, int l1, int c1);
+cudaError_t launch_pass01_fused(int l0, int c0, int l1, int c1, const PassArgs& a0, const PassArgs& a1, int g,
+                                int len2, int lag, unsigned* ctr, cudaStream_t stream);
 cudaError_t launch_pass_tma(int mode, int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t stream);
 // split-BF16 tensor-core variants (fft_tc.cu): n = 2^4 .. 2^14 in one kernel; pass lengths
 // 2^5 .. 2^12 with the default tile width pass_log_c()

@@ -69,6 +69,31 @@ __device__ __forceinline__ void st_policy(float2* p, float2 v, unsigned long lon
                  : "memory");
 }
 
+// Bounded wait until *p >= target (acquire at GPU scope), for counters that other blocks of the
+// same launch advance: ~1 us per poll, about a second in all.
+constexpr unsigned kCountWaitLimit = 1u << 20;
+__device__ __forceinline__ bool wait_count(const unsigned* p, unsigned target) {
+    for (unsigned i = 0; i < kCountWaitLimit; ++i) {
+        unsigned v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+        if (v >= target) return true;
+        __nanosleep(128);
+    }
+    return false;
+}
+
+// As wait_count, also giving up as soon as *abort is non-zero (another block's wait ran out).
+__device__ __forceinline__ bool wait_count_or_abort(const unsigned* p, unsigned target, const unsigned* abort) {
+    for (unsigned i = 0; i < kCountWaitLimit; ++i) {
+        unsigned v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+        if (v >= target) return true;
+        if (*(const volatile unsigned*)abort) return false;
+        __nanosleep(128);
+    }
+    return false;
+}
+
 // Shared memory (bytes) of a tile of 2^log_c columns of length 2^log_l, with padding.
 __host__ __device__ constexpr int smem_bytes(int log_l, int log_c) {
     return (int)sizeof(float2) * ((1 << (log_l + log_c)) + (1 << (log_l + log_c - 4)));
@@ -155,7 +180,10 @@ __device__ __forceinline__ void batched_tile(const float2* __restrict__ src, flo
 // over the 2^LOG_C L / 16 threads of the tile.
 // W: the first pass multiplies its input by a.pre, the last pass its output by a.post (see
 // PassArgs); without W they are not compiled in.
-template <int LOG_L, int LOG_C, int MODE, bool TC = false, bool W = false>
+// CG: later passes load through L2 only (ld.global.cg), for data that other blocks of the same
+// launch wrote: an SM's L1 may still hold an older copy of a line that it read for a neighbouring
+// transform.
+template <int LOG_L, int LOG_C, int MODE, bool TC = false, bool W = false, bool CG = false>
 __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long long toff, float2* smem, int tid) {
     constexpr int L = 1 << LOG_L, T = L / 16, C = 1 << LOG_C;
     const int c = tid & (C - 1);
@@ -192,7 +220,7 @@ __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long lo
         for (int k = 0; k < 16; ++k) {
             // The first pass streams the input, which is never read again. Later passes read
             // and write `out` in place, so they avoid the read-only cache path.
-            float2 x = MODE == 0 ? ld_stream(p0 + k * estep) : p0[k * estep];
+            float2 x = MODE == 0 ? ld_stream(p0 + k * estep) : CG ? __ldcg(p0 + k * estep) : p0[k * estep];
             if constexpr (W && MODE == 0) {
                 if (a.pre) x = cmul(x, __ldg(a.pre + (off0 - toff) + k * estep));
             }

@@ -139,47 +139,52 @@ constexpr int tma_min_blocks() {
                                                    : 0;
 }
 
-// One tile per block; MODE as k_pass. `tin` maps the pass's input, `tout` its output (MODE 1/2:
-// the same array, in place). Shared memory: the tile (dense as the copy lands, then reused
-// padded by the exchanges), the inter-pass twiddle factors, the mbarrier.
+// Shared memory of a TMA-staged tile, in float2 units: the tile (dense as the copy lands, then
+// reused padded by the exchanges), the inter-pass twiddle factors (17 per column); the block's
+// mbarrier follows at this offset.
+__host__ __device__ constexpr int tma_bar_offset(int log_l, int log_c) {
+    return (1 << (log_l + log_c)) + (1 << (log_l + log_c - 4)) + 17 * (1 << log_c);
+}
+__host__ __device__ constexpr int tma_smem_bytes(int log_l, int log_c) {
+    return (int)sizeof(float2) * (tma_bar_offset(log_l, log_c) + 2) + 16;
+}
+
+// One tile of a pass, MODE as k_pass, run by all threads of the block: the tile arrives through
+// one bulk tensor copy completing on the block's mbarrier `bar` (phase parity `parity`); `fresh`:
+// the barrier is initialised here (the block's first tile), else the generic accesses of the
+// block's previous tile to the landing buffer are ordered before this copy overwrites it. `tin`
+// maps the pass's input, `tout` its output (MODE 1/2: the same array, in place). Returns false,
+// the same in every thread, if the copy's bounded wait expired: the tile then recorded the
+// failure in the plan's error word, let the copy land and wrote nothing.
 // W: the first pass multiplies its input by a.pre, the last pass its output by a.post
 // (instantiated only for weighted calls).
 template <int LOG_L, int LOG_C, int MODE, bool W>
-__global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_L, LOG_C, MODE>()))
-    k_pass_tma(PassArgs a, const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout) {
+__device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* tin, const CUtensorMap* tout,
+                                         unsigned t, int b, float2* smem, uint64_t* bar, unsigned parity, bool fresh,
+                                         int tid) {
     constexpr int L = 1 << LOG_L, T = L / 16, C = 1 << LOG_C;
-    constexpr int ELO = L < 256 ? L : 256;
-    extern __shared__ __align__(1024) float2 smem[];
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + spad(C * L - 1) + 1 + 17 * C + 1);
-    const int tid = threadIdx.x;
     const int c = tid & (C - 1);
     const int j = tid >> LOG_C;
-    const unsigned t = blockIdx.x;
-    const int b = blockIdx.y;
     const unsigned col0 = a.tli >= 31 ? (t << LOG_C)
                                       : ((a.outer_base + (t >> a.tli)) << a.outer_shift) + a.inner_base +
                                             ((t & ((1u << a.tli) - 1)) << LOG_C);
     const int q0 = (int)(col0 & ((1u << a.log_s) - 1)), h = (int)(col0 >> a.log_s);
-    if (smem_u32(smem) & 127) {  // bulk tensor copies need a 128-byte aligned destination
-        if (tid == 0) *(volatile unsigned*)a.err = 2u;
-        return;
-    }
     if (tid == 0) {
-        mbar_init(bar, 1);
+        if (fresh) mbar_init(bar, 1);
+        else asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_expect_tx(bar, (unsigned)(C * L * sizeof(float2)));
         // With l2_keep the array between passes should stay in L2: the input (read once) and
         // the last pass's tile (read for the last time) are loaded evict-first.
         if (a.l2_keep && MODE != 1) {
             const unsigned long long first = policy_evict_first();
-            if (MODE == 0) tma_load_4d_hint(smem, &tin, (int)col0, 0, 0, b, bar, first);
-            else tma_load_5d_hint(smem, &tin, q0, 0, 0, h, b, bar, first);
+            if (MODE == 0) tma_load_4d_hint(smem, tin, (int)col0, 0, 0, b, bar, first);
+            else tma_load_5d_hint(smem, tin, q0, 0, 0, h, b, bar, first);
         } else if (MODE == 0) {
-            tma_load_4d(smem, &tin, (int)col0, 0, 0, b, bar);
+            tma_load_4d(smem, tin, (int)col0, 0, 0, b, bar);
         } else {
-            tma_load_5d(smem, &tin, q0, 0, 0, h, b, bar);
+            tma_load_5d(smem, tin, q0, 0, 0, h, b, bar);
         }
     }
-    (void)ELO;
     // inter-pass twiddle factors (as pass_tile) while the copy is in flight
     float2* tws = smem + spad(C * L - 1) + 1;
     float2 wjf = make_float2(1.f, 0.f);
@@ -187,14 +192,14 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_
         pass_twiddle_rows<LOG_L, LOG_C, MODE>(a, col0, tws, tid, C * T);
         wjf = pass_twiddle_lane<LOG_L>(a, MODE == 0 ? col0 + c : (col0 >> a.log_s) << a.log_s, j);
     }
-    __syncthreads();  // the barrier is initialised before anyone waits on it
-    const bool ok = !g_expire_waits && mbar_wait(bar, 0);
+    __syncthreads();  // the barrier is initialised (and armed) before anyone waits on it
+    const bool ok = !g_expire_waits && mbar_wait(bar, parity);
     if (__syncthreads_or(!ok)) {
         if (tid == 0) {
             *(volatile unsigned*)a.err = 1u;
-            mbar_wait(bar, 0);  // let a late copy land before the block's memory is released
+            mbar_wait(bar, parity);  // let a late copy land before the memory is reused or released
         }
-        return;
+        return false;
     }
     float2 v[16];
 #pragma unroll
@@ -227,7 +232,6 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_
         const unsigned j2 = rr & ((1u << a.rev_b2) - 1), j1 = rr >> a.rev_b2;
         float2* q = a.out + ((long long)b << a.log2n) + (((j1 + (j2 << a.rev_b1)) << LOG_L) + kk0);
         const float2* r = smem + spad(kk0 * C + cc);
-#pragma unroll
         if (a.l2_keep) {
             const unsigned long long keep = policy_evict_last();  // the next pass reads these
 #pragma unroll
@@ -252,9 +256,148 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
-            if (MODE == 1 && a.l2_keep) tma_store_5d_hint(&tout, smem, q0, 0, 0, h, b, policy_evict_last());
-            else tma_store_5d(&tout, smem, q0, 0, 0, h, b);
+            if (MODE == 1 && a.l2_keep) tma_store_5d_hint(tout, smem, q0, 0, 0, h, b, policy_evict_last());
+            else tma_store_5d(tout, smem, q0, 0, 0, h, b);
         }
+    }
+    return true;
+}
+
+// One tile per block (blockIdx.x the tile, blockIdx.y the transform of the batch).
+template <int LOG_L, int LOG_C, int MODE, bool W>
+__global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_L, LOG_C, MODE>()))
+    k_pass_tma(PassArgs a, const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout) {
+    extern __shared__ __align__(1024) float2 smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + tma_bar_offset(LOG_L, LOG_C));
+    if (smem_u32(smem) & 127) {  // bulk tensor copies need a 128-byte aligned destination
+        if (threadIdx.x == 0) *(volatile unsigned*)a.err = 2u;
+        return;
+    }
+    tma_tile<LOG_L, LOG_C, MODE, W>(a, &tin, &tout, blockIdx.x, (int)blockIdx.y, smem, bar, 0u, true,
+                                    (int)threadIdx.x);
+}
+
+// ---- passes 0 and 1 of a three-pass transform in one persistent launch -----------------------
+//
+// n = A B C (pass lengths 2^len[0..2]). Pass 1 on the columns of last digit j_c needs only pass
+// 0's outputs for the same j_c, and those form one contiguous region of A B 2^g values per
+// chunk of 2^g digits (see plan_enqueue's chunked launches). Here one launch runs both passes,
+// chunk by chunk: blocks take tiles in order from a device counter, a sequence that issues
+// pass 0 of chunk k + lag before pass 1 of chunk k; a pass-1 tile first waits (bounded) until
+// every pass-0 tile of its chunk has published its stores. A chunk's intermediate values are then
+// re-read from L2 a few microseconds after they were written, instead of from HBM after the whole
+// array went through pass 0, so passes 0 and 1 together move the array through HBM once (read
+// the input, write the result) instead of twice. The tile arithmetic is tma_tile's, so results
+// equal the separate passes bit for bit.
+//
+// Counters (one slot per launch, zero at entry; the last block to leave zeroes them again):
+// [0] the next tile of the sequence, [1] blocks that have left, [2 + k] pass-0 tiles of chunk k
+// published.
+struct FusedArgs {
+    PassArgs p0;      // pass 0 (inner_base: the chunk's first last-digit column, set per tile)
+    PassArgs p1;      // pass 1 (outer_base: the same, set per tile)
+    int g;            // log2 last-digit columns per chunk
+    unsigned chunks;  // 2^(len[2] - g)
+    unsigned lag;     // chunks by which pass 1 trails pass 0 (1 <= lag <= chunks)
+    unsigned t0, t1;  // tiles per chunk of pass 0 and of pass 1
+    unsigned total;   // chunks (t0 + t1)
+    unsigned* ctr;
+};
+
+// Tile s of the sequence: `lag` chunks of pass 0, then per chunk k pass 0 of chunk k + lag
+// followed by pass 1 of chunk k, then the last `lag` chunks of pass 1.
+__device__ __forceinline__ void fused_decode(const FusedArgs& f, unsigned s, int& pass, unsigned& chunk,
+                                             unsigned& tile) {
+    const unsigned pre = f.lag * f.t0;
+    if (s < pre) {
+        pass = 0, chunk = s / f.t0, tile = s % f.t0;
+        return;
+    }
+    s -= pre;
+    const unsigned step = f.t0 + f.t1, mid = (f.chunks - f.lag) * step;
+    if (s < mid) {
+        const unsigned k = s / step, r = s % step;
+        if (r < f.t0) pass = 0, chunk = k + f.lag, tile = r;
+        else pass = 1, chunk = k, tile = r - f.t0;
+        return;
+    }
+    s -= mid;
+    pass = 1, chunk = f.chunks - f.lag + s / f.t1, tile = s % f.t1;
+}
+
+// Both tile shapes run with the same number of threads: 2^(L0 + C0 - 4) = 2^(L1 + C1 - 4).
+template <int L0, int C0, int L1, int C1>
+constexpr int fused_min_blocks() {
+    return L0 == 8 && C0 == 4 && L1 == 9 && C1 == 3 ? 5 : 0;
+}
+
+template <int L0, int C0, int L1, int C1>
+__global__ void __launch_bounds__(1 << (L0 + C0 - 4), (fused_min_blocks<L0, C0, L1, C1>()))
+    k_pass01_fused(FusedArgs f, const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tmid) {
+    static_assert(L0 + C0 == L1 + C1, "both passes' tiles need the same threads");
+    constexpr int BAR = tma_bar_offset(L0, C0) > tma_bar_offset(L1, C1) ? tma_bar_offset(L0, C0)
+                                                                        : tma_bar_offset(L1, C1);
+    extern __shared__ __align__(1024) float2 smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + BAR);
+    unsigned* shared_word = reinterpret_cast<unsigned*>(smem + BAR + 1);  // the next tile, then "last block"
+    const int tid = threadIdx.x;
+    if (smem_u32(smem) & 127) {  // bulk tensor copies need a 128-byte aligned destination
+        if (tid == 0) *(volatile unsigned*)f.p0.err = 2u;
+    } else {
+        if (tid == 0) *shared_word = atomicAdd(f.ctr, 1u);
+        __syncthreads();
+        unsigned s = *shared_word, parity = 0;
+        bool fresh = true;
+        while (s < f.total) {
+            int pass;
+            unsigned chunk, tile;
+            fused_decode(f, s, pass, chunk, tile);
+            __syncthreads();  // every thread has read the next-tile word
+            if (tid == 0) *shared_word = atomicAdd(f.ctr, 1u);  // fetched while this tile runs
+            bool ok;
+            if (pass == 0) {
+                PassArgs a = f.p0;
+                a.inner_base = chunk << f.g;
+                ok = tma_tile<L0, C0, 0, false>(a, &tin, &tin, tile, 0, smem, bar, parity, fresh, tid);
+                __syncthreads();  // every thread's stores of the tile are issued
+                if (ok && tid == 0) {
+                    __threadfence();  // ... and visible at GPU scope before the count says so
+                    atomicAdd(f.ctr + 2 + chunk, 1u);
+                }
+            } else {
+                bool ready = true;
+                if (tid == 0) {
+                    ready = !g_expire_waits && wait_count(f.ctr + 2 + chunk, f.t0);
+                    // the chunk's values were written by other blocks through the generic proxy;
+                    // this block reads them with a bulk tensor copy (the async proxy)
+                    asm volatile("fence.proxy.async.global;" ::: "memory");
+                    if (!ready) *(volatile unsigned*)f.p1.err = 3u;
+                }
+                ok = !__syncthreads_or(!ready);
+                if (ok) {
+                    PassArgs a = f.p1;
+                    a.outer_base = chunk << f.g;
+                    ok = tma_tile<L1, C1, 1, false>(a, &tmid, &tmid, tile, 0, smem, bar, parity, fresh, tid);
+                }
+            }
+            if (!ok) break;  // block-uniform: an expired wait, recorded in the error word
+            parity ^= 1u;
+            fresh = false;
+            __syncthreads();  // the next-tile word is written; the tile's shared memory is free
+            s = *shared_word;
+        }
+    }
+    // The last block to leave zeroes the counters for the next launch on this slot: every other
+    // block has left its loop, so none touches them again.
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        *shared_word = atomicAdd(f.ctr + 1, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (*shared_word) {
+        for (unsigned k = tid; k < f.chunks + 2; k += blockDim.x) f.ctr[k] = 0;
+        __threadfence();
     }
 }
 
@@ -305,7 +448,7 @@ static bool make_map(CUtensorMap* m, const float2* base, int mode, int log2n, in
 template <int LOG_L, int LOG_C, int MODE, bool W>
 static cudaError_t launch_tma_w(const PassArgs& a, int batch, cudaStream_t stream) {
     constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
-    constexpr int SMEM = smem_bytes(LOG_L, LOG_C) + (int)sizeof(float2) * (17 * (1 << LOG_C) + 2) + 16;
+    constexpr int SMEM = tma_smem_bytes(LOG_L, LOG_C);
     auto kernel = k_pass_tma<LOG_L, LOG_C, MODE, W>;
     static std::atomic<unsigned long long> done{0};
     const cudaError_t attr = smem_limit((const void*)kernel, SMEM, done);
@@ -375,6 +518,80 @@ cudaError_t launch_pass_tma(int mode, int log_l, int log_c, const PassArgs& a, i
     case 1: return launch_tma_mode<1>(log_l, log_c, a, batch, stream);
     default: return launch_tma_mode<2>(log_l, log_c, a, batch, stream);
     }
+}
+
+}  // namespace ofb
+
+namespace ofb {
+
+// ---- fused passes 0+1: host side ----------------------------------------------------------------
+
+// Shapes (L0, C0, L1, C1) with a fused kernel: both tiles have a TMA kernel and the same threads.
+#define OFB_FUSED_SHAPES(X) \
+    X(8, 4, 9, 3)           \
+    X(8, 3, 8, 3)           \
+    X(8, 4, 8, 4)           \
+    X(8, 3, 7, 4)           \
+    X(9, 3, 9, 3)           \
+    X(10, 3, 10, 3)         \
+    X(10, 3, 11, 2)
+
+bool pass01_fused_supported(int l0, int c0, int l1, int c1) {
+#define OFB_FUSED_MATCH(A0, B0, A1, B1) \
+    if (l0 == A0 && c0 == B0 && l1 == A1 && c1 == B1) return true;
+    OFB_FUSED_SHAPES(OFB_FUSED_MATCH)
+#undef OFB_FUSED_MATCH
+    return false;
+}
+
+template <int L0, int C0, int L1, int C1>
+static cudaError_t launch_fused_t(const FusedArgs& f, int log2n, cudaStream_t stream) {
+    constexpr int THREADS = 1 << (L0 + C0 - 4);
+    constexpr int SMEM = tma_smem_bytes(L0, C0) > tma_smem_bytes(L1, C1) ? tma_smem_bytes(L0, C0)
+                                                                        : tma_smem_bytes(L1, C1);
+    auto kernel = k_pass01_fused<L0, C0, L1, C1>;
+    static std::atomic<unsigned long long> done{0};
+    cudaError_t e = smem_limit((const void*)kernel, SMEM, done);
+    if (e != cudaSuccess) return e;
+    // persistent grid: as many blocks as fit on the device at once (per device, computed once)
+    static std::atomic<int> grid_of[64];
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    int grid = grid_of[dev & 63].load(std::memory_order_relaxed);
+    if (grid == 0) {
+        int per_sm = 0, sms = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, THREADS, SMEM)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        grid = per_sm * sms > 0 ? per_sm * sms : 1;
+        grid_of[dev & 63].store(grid, std::memory_order_relaxed);
+    }
+    if ((unsigned)grid > f.total) grid = (int)f.total;
+    CUtensorMap tin, tmid;
+    if (!make_map(&tin, f.p0.in, 0, log2n, L0, C0, f.p0.log_s, 1) ||
+        !make_map(&tmid, f.p1.out, 1, log2n, L1, C1, f.p1.log_s, 1))
+        return cudaErrorInvalidValue;
+    kernel<<<grid, THREADS, SMEM, stream>>>(f, tin, tmid);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pass01_fused(int l0, int c0, int l1, int c1, const PassArgs& a0, const PassArgs& a1, int g,
+                                int len2, int lag, unsigned* ctr, cudaStream_t stream) {
+    if (!pass01_fused_supported(l0, c0, l1, c1) || g < c0 || g > len2) return cudaErrorInvalidValue;
+    FusedArgs f{};
+    f.p0 = a0;
+    f.p1 = a1;
+    f.g = g;
+    f.chunks = 1u << (len2 - g);
+    f.lag = lag < 1 ? 1u : (unsigned)lag > f.chunks ? f.chunks : (unsigned)lag;
+    f.t0 = a0.ntiles;
+    f.t1 = a1.ntiles;
+    f.total = f.chunks * (f.t0 + f.t1);
+    f.ctr = ctr;
+#define OFB_FUSED_CASE(A0, B0, A1, B1) \
+    if (l0 == A0 && c0 == B0 && l1 == A1 && c1 == B1) return launch_fused_t<A0, B0, A1, B1>(f, a0.log2n, stream);
+    OFB_FUSED_SHAPES(OFB_FUSED_CASE)
+#undef OFB_FUSED_CASE
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace ofb

@@ -83,6 +83,15 @@ static bool size_log2(size_t n, int *log2n) {
 
 // ---- plans -------------------------------------------------------------------------------------
 
+// Counter slot of the fused pass-0/1 kernel: launches that take the same slot are ordered by
+// its event (the slot's previous launch has finished and left the counters zeroed).
+struct FusedSlot {
+    std::mutex m;
+    cudaEvent_t done = nullptr;
+    bool used = false;
+};
+constexpr int kFusedSlots = 4;
+
 struct onefft_plan {
     size_t n;
     int log2n;
@@ -95,6 +104,12 @@ struct onefft_plan {
     int chunk;             // three passes: log2 of the last-digit columns per chunk of passes 0+1 (0 = none)
     int tc;                // radix-16 stages as split-BF16 tensor-core products (onefft_plan_create_bf16x3)
     int tma;               // passes staged through bulk tensor copies where the tile shape has a TMA kernel
+    int fuse_lag;          // three passes, chunked: passes 0+1 as one persistent launch with pass 1
+                           // trailing by this many chunks (0 = separate launches)
+    unsigned *fused_ctr;   // kFusedSlots counter slots of fused_words words each, in `mem`
+    size_t fused_words;
+    FusedSlot *slots;
+    mutable std::atomic<unsigned> next_slot{0};
     unsigned *err;         // error word as kernels address it: set by a kernel whose bounded wait ran out
     unsigned *err_host;    // the same word on the host (mapped pinned memory: read without a copy)
     void *mem;             // the one device allocation
@@ -115,6 +130,7 @@ struct Shape {
     int l2_keep;
     int chunk;
     int tma;
+    int fuse_lag;
 };
 
 // Fastest shapes measured on a B200 by onefft_b200/autotune.py (forward transform, L2 flushed
@@ -176,6 +192,10 @@ static bool valid_shape(int m, const Shape &s) {
     // and a chunk holds whole first-pass tiles
     if (s.npass == 3 && s.cols[0] > s.len[2]) return false;
     if (s.chunk && (s.npass != 3 || s.chunk < s.cols[0] || s.chunk > s.len[2])) return false;
+    // the fused passes 0+1 need chunks, bulk tensor copies and a compiled tile pair
+    if (s.fuse_lag && (!s.chunk || !s.tma || s.fuse_lag > 15 ||
+                       !pass01_fused_supported(s.len[0], s.cols[0], s.len[1], s.cols[1])))
+        return false;
     return sum == m;
 }
 
@@ -200,6 +220,7 @@ static onefft_plan *plan_build(size_t n, int m, const Shape &shape) {
     p->l2_keep = shape.l2_keep;
     p->chunk = shape.chunk;
     p->tma = shape.tma;
+    p->fuse_lag = shape.fuse_lag;
     for (int i = 0; i < shape.npass; ++i) {
         p->len[i] = shape.len[i];
         p->cols[i] = shape.cols[i];
@@ -218,8 +239,20 @@ static onefft_plan *plan_build(size_t n, int m, const Shape &shape) {
         hi_off = bytes;
         bytes = align256(bytes + sizeof(double2) * ((size_t)1 << (m - p->lo_bits)));
     }
+    size_t ctr_off = bytes;
+    if (p->fuse_lag) {  // counter slots of the fused passes: next tile, blocks done, one per chunk
+        p->fused_words = align256(sizeof(unsigned) * (2 + ((size_t)1 << (p->len[2] - p->chunk)))) / sizeof(unsigned);
+        bytes += kFusedSlots * p->fused_words * sizeof(unsigned);
+        p->slots = new (std::nothrow) FusedSlot[kFusedSlots];
+        if (!p->slots) {
+            delete p;
+            set_error(ONEFFT_ERR_SIZE, "out of host memory");
+            return nullptr;
+        }
+    }
     e = dev_alloc(&p->mem, bytes);
     if (e != cudaSuccess) {
+        delete[] p->slots;
         delete p;
         cuda_error(e, "plan table allocation");
         set_error(ONEFFT_ERR_SIZE, "plan table allocation failed");
@@ -250,6 +283,12 @@ static onefft_plan *plan_build(size_t n, int m, const Shape &shape) {
             p->tw_hi = (const double2 *)(base + hi_off);
             e = launch_big_table((double2 *)p->tw_lo, (double2 *)p->tw_hi, m, p->lo_bits, s);
         }
+        if (p->fuse_lag && e == cudaSuccess) {
+            p->fused_ctr = (unsigned *)(base + ctr_off);
+            e = cudaMemsetAsync(p->fused_ctr, 0, kFusedSlots * p->fused_words * sizeof(unsigned), s);
+            for (int i = 0; i < kFusedSlots && e == cudaSuccess; ++i)
+                e = cudaEventCreateWithFlags(&p->slots[i].done, cudaEventDisableTiming);
+        }
         cudaError_t e2 = cudaStreamSynchronize(s);
         if (e == cudaSuccess) e = e2;
         cudaStreamDestroy(s);
@@ -257,6 +296,10 @@ static onefft_plan *plan_build(size_t n, int m, const Shape &shape) {
     if (e != cudaSuccess) {
         cudaFree(p->mem);
         if (p->err_host) cudaFreeHost(p->err_host);
+        if (p->slots)
+            for (int i = 0; i < kFusedSlots; ++i)
+                if (p->slots[i].done) cudaEventDestroy(p->slots[i].done);
+        delete[] p->slots;
         delete p;
         cuda_error(e, "plan table build");
         return nullptr;
@@ -289,6 +332,7 @@ extern "C" onefft_plan *onefft_plan_create_tiles(size_t n, int npass, const int 
     s.l2_keep = (options & ONEFFT_OPT_L2_KEEP) ? 1 : 0;
     s.tma = (options & ONEFFT_OPT_TMA) ? 1 : 0;
     s.chunk = log2_chunk > 0 ? log2_chunk : 0;
+    if (options & ONEFFT_OPT_FUSED) s.fuse_lag = ((options >> 8) & 15) ? ((options >> 8) & 15) : 1;
     for (int i = 0; i < npass; ++i) {
         s.len[i] = log2_len[i];
         s.cols[i] = log2_cols ? log2_cols[i] : pass_log_c(log2_len[i]);
@@ -321,6 +365,7 @@ extern "C" onefft_plan *onefft_plan_create_bf16x3(size_t n, int require_accepted
     Shape s = tuned_shape(m);
     s.chunk = 0;
     s.tma = 0;
+    s.fuse_lag = 0;
     for (int i = 0; i < s.npass; ++i) {
         s.cols[i] = pass_log_c(s.len[i]);
         if (s.npass > 1 && s.len[i] < 5) {
@@ -344,6 +389,10 @@ extern "C" void onefft_plan_destroy(onefft_plan *plan) {
     if (cur != plan->device) cudaSetDevice(plan->device);
     cudaFree(plan->mem);
     if (plan->err_host) cudaFreeHost(plan->err_host);
+    if (plan->slots)
+        for (int i = 0; i < kFusedSlots; ++i)
+            if (plan->slots[i].done) cudaEventDestroy(plan->slots[i].done);
+    delete[] plan->slots;
     if (cur >= 0 && cur != plan->device) cudaSetDevice(cur);
     delete plan;
 }
@@ -395,6 +444,62 @@ static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *
         return p->tc ? launch_pass_tc(mode, p->len[i], x, (int)batch, s)
                      : launch_pass(mode, p->len[i], p->cols[i], x, (int)batch, s);
     };
+    if (p->npass == 3 && p->fuse_lag && use_tma && !pre) {
+        // Passes 0 and 1 in one persistent launch per transform (k_pass01_fused), then pass 2
+        // over the batch. The launch needs a counter slot that no launch running at the same
+        // time uses: slots are taken in turn, and a slot's next launch waits on the GPU for the
+        // event recorded after its previous one. Stream capture would record that wait on an
+        // event from outside the graph, so captured calls take the separate launches below.
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) {
+            cudaGetLastError();
+            cs = cudaStreamCaptureStatusActive;
+        }
+        if (cs == cudaStreamCaptureStatusNone) {
+            const int A = p->len[0], B = p->len[1], Cd = p->len[2], G = p->chunk;
+            PassArgs c0 = a, c1 = a;
+            c0.stw = p->stw[0];
+            c0.swap_in = inverse;
+            c0.swap_out = 0;
+            c0.log_s = p->log2n - A;
+            c0.rev_b1 = B;
+            c0.rev_b2 = Cd;
+            c0.tli = G - p->cols[0];
+            c0.outer_shift = Cd;
+            c0.outer_base = 0;
+            c0.ntiles = 1u << (B + G - p->cols[0]);
+            c1.stw = p->stw[1];
+            c1.swap_in = c1.swap_out = 0;
+            c1.log_s = A;
+            c1.tli = A - p->cols[1];
+            c1.outer_shift = A;
+            c1.inner_base = 0;
+            c1.ntiles = 1u << (G + A - p->cols[1]);
+            const unsigned k = p->next_slot.fetch_add(1, std::memory_order_relaxed) % kFusedSlots;
+            FusedSlot &slot = p->slots[k];
+            std::lock_guard<std::mutex> lock(slot.m);
+            cudaError_t e = slot.used ? cudaStreamWaitEvent(s, slot.done, 0) : cudaSuccess;
+            for (long long b = 0; b < batch && e == cudaSuccess; ++b) {
+                c0.in = in + (b << p->log2n);
+                c0.out = c1.out = out + (b << p->log2n);
+                c1.in = c1.out;
+                g_launches.fetch_add(1);
+                e = launch_pass01_fused(A, p->cols[0], B, p->cols[1], c0, c1, G, Cd, p->fuse_lag,
+                                        p->fused_ctr + k * p->fused_words, s);
+            }
+            if (e == cudaSuccess) e = cudaEventRecord(slot.done, s);
+            if (e != cudaSuccess) return e;
+            slot.used = true;
+            a.in = out;
+            a.out = out;
+            a.stw = p->stw[2];
+            a.swap_in = 0;
+            a.swap_out = inverse;
+            a.log_s = A + B;
+            g_launches.fetch_add(1);
+            return run(2, 2, a);
+        }
+    }
     if (p->npass == 3 && p->chunk > 0) {
         // Passes 0 and 1 of a three-pass transform n = A B C run chunk by chunk over the last
         // digit j_c: pass 1 on columns j_c needs only pass 0's outputs for the same j_c, which
