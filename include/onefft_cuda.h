@@ -153,8 +153,13 @@ ONEFFT_API void onefft_uneven_destroy(onefft_uneven *batch);
 ONEFFT_API size_t onefft_uneven_span(const onefft_uneven *batch);
 /* Runs the whole batch from d_in to d_out (device buffers of at least onefft_uneven_span()
  * complex values, 8-byte aligned, not overlapping) on `stream`. The batch object holds the work
- * queue counter, so one batch object must not execute on two streams at once. */
+ * queue counters, so one batch object must not execute on two streams at once. */
 ONEFFT_API int onefft_uneven_execute(onefft_uneven *batch, const float *d_in, float *d_out, void *stream);
+/* As onefft_plan_status for a batch: the second pass of a transform of 2^13 .. 2^16 waits
+ * (bounded) for its first pass, which other blocks run; if that wait ran out, the batch's output
+ * is not valid. Returns 0, or ONEFFT_ERR_CUDA_BASE with the reason in onefft_last_error();
+ * reading clears it. Call after synchronising the stream of the execute calls. */
+ONEFFT_API int onefft_uneven_status(onefft_uneven *batch);
 
 /* The same uneven batch with no device allocation at all, for callers that cannot let a library
  * call cudaMalloc: real-time threads that must not block in the allocator or hit out-of-memory

@@ -35,6 +35,7 @@ C_SYMBOLS = (
     "onefft_plan_forward_batched", "onefft_plan_inverse_batched",
     "onefft_plan_create_split", "onefft_plan_create_tiles", "onefft_plan_create_bf16x3", "onefft_plan_passes",
     "onefft_uneven_create", "onefft_uneven_create_split", "onefft_uneven_destroy", "onefft_uneven_span", "onefft_uneven_execute",
+    "onefft_uneven_status",
     "onefft_uneven_execute_noalloc",
     "onefft_last_error", "onefft_plan_status", "onefft_debug_fail_alloc", "onefft_debug_twiddles",
     "onefft_debug_launch_count", "onefft_debug_expire_waits",
@@ -105,6 +106,8 @@ def lib() -> ctypes.CDLL:
     L.onefft_uneven_span.restype = _sz
     L.onefft_uneven_execute.argtypes = [_vp, _vp, _vp, _vp]
     L.onefft_uneven_execute.restype = ctypes.c_int
+    L.onefft_uneven_status.argtypes = [_vp]
+    L.onefft_uneven_status.restype = ctypes.c_int
     L.onefft_uneven_execute_noalloc.argtypes = [_vp, _sz, _vp, _vp, _vp]
     L.onefft_uneven_execute_noalloc.restype = ctypes.c_int
     L.onefft_last_error.argtypes = []
@@ -337,6 +340,10 @@ class UnevenBatch:
         rc = lib().onefft_uneven_execute(self._h, d_in, d_out, stream)
         if rc != 0:
             raise RuntimeError(f"onefft_uneven_execute failed ({rc}): {last_error()}")
+
+    def status(self) -> int:
+        """onefft_uneven_status: 0, or the error code of a failed wait since the last call."""
+        return int(lib().onefft_uneven_status(self._h))
 
     def destroy(self) -> None:
         if getattr(self, "_h", None):

@@ -938,7 +938,8 @@ struct onefft_uneven {
     size_t count;
     size_t span;
     onefft_plan *plans[kUnevenMaxLog2 + 1];
-    void *mem;  // sorted descriptors, work items, queue counter
+    void *mem;  // sorted descriptors, work items, units, queue counter + per-item step counters
+    unsigned *err_host;  // error word (mapped pinned host memory), as the plans'
     UnevenArgs args;
     int grid;
     int smem;
@@ -952,11 +953,48 @@ extern "C" void onefft_uneven_destroy(onefft_uneven *u) {
     if (u->exec) cudaGraphExecDestroy(u->exec);
     if (u->graph) cudaGraphDestroy(u->graph);
     if (u->mem) cudaFree(u->mem);
+    if (u->err_host) cudaFreeHost(u->err_host);
     for (int m = 0; m <= kUnevenMaxLog2; ++m) onefft_plan_destroy(u->plans[m]);
     delete u;
 }
 
 extern "C" size_t onefft_uneven_span(const onefft_uneven *u) { return u ? u->span : 0; }
+
+extern "C" int onefft_uneven_status(onefft_uneven *u) {
+    t_last_error.clear();
+    if (!u) return set_error(ONEFFT_ERR_ARG, "NULL batch");
+    volatile unsigned *word = u->err_host;
+    const unsigned flag = *word;
+    if (!flag) return 0;
+    *word = 0;
+    return set_error(ONEFFT_ERR_CUDA_BASE, "a pass-1 step waited too long for its pass 0 (code %u)", flag);
+}
+
+// Queue order of the step-wise uneven kernel: each transform of 2^13 .. 2^16 (largest first) as
+// its pass-0 steps, its pass-1 steps placed at least kUnevenLagUnits units later (so they rarely
+// wait, and the values between the passes of the transforms in flight stay in L2); then every
+// smaller item whole.
+static std::vector<UnevenUnit> uneven_units(const std::vector<UnevenItem> &items) {
+    std::vector<UnevenUnit> units;
+    std::vector<std::pair<int, size_t>> pending;  // (item, queue length after its pass 0)
+    size_t head = 0;
+    auto emit_pass1 = [&](int i) {
+        const int steps = 1 << (items[i].log2n - 12);
+        for (int k = 0; k < steps; ++k) units.push_back(UnevenUnit{i, steps + k});
+    };
+    for (int i = 0; i < (int)items.size(); ++i) {
+        if (items[i].log2n < 13) continue;
+        const int steps = 1 << (items[i].log2n - 12);
+        for (int k = 0; k < steps; ++k) units.push_back(UnevenUnit{i, k});
+        pending.emplace_back(i, units.size());
+        while (head < pending.size() && units.size() - pending[head].second >= (size_t)kUnevenLagUnits)
+            emit_pass1(pending[head++].first);
+    }
+    while (head < pending.size()) emit_pass1(pending[head++].first);
+    for (int i = 0; i < (int)items.size(); ++i)
+        if (items[i].log2n < 13) units.push_back(UnevenUnit{i, -1});
+    return units;
+}
 
 static onefft_uneven *uneven_create(const onefft_desc *desc, size_t count, const int *split_choice);
 
@@ -1063,23 +1101,40 @@ static onefft_uneven *uneven_create(const onefft_desc *desc, size_t count, const
         u->args.tw_hi[m] = p->tw_hi;
         u->args.lo_bits[m] = p->lo_bits;
     }
+    const std::vector<UnevenUnit> units = uneven_units(items);
     const size_t desc_bytes = align256(count * sizeof(onefft_desc));
     const size_t item_bytes = align256(items.size() * sizeof(UnevenItem));
-    e = dev_alloc(&u->mem, desc_bytes + item_bytes + 256);
+    const size_t unit_bytes = align256(units.size() * sizeof(UnevenUnit));
+    // queue head, per item the pass-0 steps done, the abort word
+    const size_t ctr_bytes = sizeof(int) + sizeof(unsigned) * (items.size() + 1);
+    e = dev_alloc(&u->mem, desc_bytes + item_bytes + unit_bytes + align256(ctr_bytes));
     if (e != cudaSuccess) {
         u->mem = nullptr;
         onefft_uneven_destroy(u);
         set_error(ONEFFT_ERR_SIZE, "uneven batch allocation failed");
         return nullptr;
     }
+    e = cudaHostAlloc((void **)&u->err_host, sizeof(unsigned), cudaHostAllocMapped | cudaHostAllocPortable);
+    if (e == cudaSuccess) {
+        *(volatile unsigned *)u->err_host = 0;
+        e = cudaHostGetDevicePointer((void **)&u->args.err, u->err_host, 0);
+    } else {
+        u->err_host = nullptr;
+    }
     char *base = (char *)u->mem;
     u->args.desc = (const onefft_desc *)base;
     u->args.items = (const UnevenItem *)(base + desc_bytes);
-    u->args.counter = (int *)(base + desc_bytes + item_bytes);
+    u->args.units = (const UnevenUnit *)(base + desc_bytes + item_bytes);
+    u->args.nunits = (int)units.size();
+    u->args.counter = (int *)(base + desc_bytes + item_bytes + unit_bytes);
+    u->args.done = (unsigned *)(u->args.counter + 1);
     u->args.nitems = (int)items.size();
-    e = cudaMemcpy(base, sorted.data(), count * sizeof(onefft_desc), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(base, sorted.data(), count * sizeof(onefft_desc), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = cudaMemcpy(base + desc_bytes, items.data(), items.size() * sizeof(UnevenItem), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(base + desc_bytes + item_bytes, units.data(), units.size() * sizeof(UnevenUnit),
+                       cudaMemcpyHostToDevice);
     // persistent grid: every block resident at once
     u->smem = uneven_smem_bytes();
     int per_sm = 0, sms = 0;
@@ -1088,7 +1143,8 @@ static onefft_uneven *uneven_create(const onefft_desc *desc, size_t count, const
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, uneven_kernel(u->args.split), 256, u->smem);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     u->grid = std::max(1, std::min(per_sm * sms, (int)items.size()));
-    // graph: zero the queue counter, then the persistent launch
+    // graph: zero the queue counter, the per-item step counters and the abort word, then the
+    // persistent launch
     if (e == cudaSuccess) e = cudaGraphCreate(&u->graph, 0);
     cudaGraphNode_t mset = nullptr;
     if (e == cudaSuccess) {
@@ -1096,7 +1152,7 @@ static onefft_uneven *uneven_create(const onefft_desc *desc, size_t count, const
         mp.dst = u->args.counter;
         mp.value = 0;
         mp.elementSize = 4;
-        mp.width = 1;
+        mp.width = 2 + items.size();
         mp.height = 1;
         e = cudaGraphAddMemsetNode(&mset, u->graph, nullptr, 0, &mp);
     }

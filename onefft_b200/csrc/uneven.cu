@@ -9,8 +9,14 @@
 //     16 <= n <= 4096 (one block tile, the plain path's batched tile), or one transform of
 //     2^13 .. 2^16 (both passes of a two-pass split run by the same block, tile after tile, with
 //     the intermediate values in `out`, i.e. in L2);
-//   - k_uneven: every block loops, taking the next work item from a device counter, until the
-//     queue is empty. No block ever waits for another.
+//   - k_uneven: every block loops, taking the next unit of work from a device counter, until the
+//     queue is empty. A transform of 2^13 .. 2^16 is split into steps of 4096 values (its pass-0
+//     tiles, then its pass-1 tiles) that any block may take; a pass-1 step waits (bounded) on a
+//     per-transform counter of finished pass-0 steps, and the queue places it at least
+//     kUnevenLagUnits units after them, so it rarely waits. Many blocks then share the few
+//     transforms in flight, and the values between their passes stay in L2, where one block per
+//     transform kept hundreds of megabytes of them in flight. (With no unit queue, as in
+//     onefft_uneven_execute_noalloc, every block runs whole transforms; the same bits either way.)
 //   - the memset of the counter plus the launch form a CUDA graph built at creation; execute
 //     patches the buffer pointers into the kernel node and replays it.
 // Per work item the arithmetic is the plain path's tile body (fft_tiles.cuh) with the plain
@@ -109,6 +115,67 @@ __device__ __forceinline__ void big_item(const BigItemArgs& b, float2* smem, int
     }
 }
 
+// One step (4096 values) of a 2^M transform split 2^L0 x 2^L1, for the step-wise queue: steps
+// 0 .. S - 1 run tiles of pass 0 and publish them in the item's counter; steps S .. 2S - 1 run
+// tiles of pass 1 once every pass-0 step of the item is published (bounded wait). S = 2^(M - 12).
+// The tiles are the ones big_item runs, with the same arithmetic, so results are the same bits.
+template <int M, int L0, int L1>
+__device__ __forceinline__ void big_step(const BigItemArgs& b, unsigned* done, unsigned* abort, unsigned* err, int step,
+                                         float2* smem, int tid) {
+    constexpr int S = 1 << (M - 12);
+    PassArgs p{};
+    p.in = b.in;
+    p.out = b.out;
+    p.log2n = M;
+    p.tw_lo = b.tw_lo;
+    p.tw_hi = b.tw_hi;
+    p.lo_bits = b.lo_bits;
+    p.tli = 31;
+    if (step < S) {
+        constexpr int LC = inblock_log_c(L0), TT = 1 << (L0 + LC - 4), G = kUnevenThreads / TT;
+        p.log_s = M - L0;
+        p.rev_b1 = L1;
+        p.rev_b2 = 0;
+        p.swap_in = b.inverse;
+        p.swap_out = 0;
+        p.stw = b.stw0;
+        float2* sm = smem + (tid / TT) * (pass_smem_bytes(L0, LC, 0) / (int)sizeof(float2));
+        pass_tile<L0, LC, 0>(p, (unsigned)(step * G + tid / TT), 0, sm, tid % TT);
+        __syncthreads();  // every thread's stores of the step are issued
+        if (tid == 0) {
+            __threadfence();  // ... and visible at GPU scope before the count says so
+            atomicAdd(done, 1u);
+        }
+    } else {
+        bool ready = true;
+        if (tid == 0) {
+            // abort: the word after the last item's counter, set by the first wait that runs
+            // out, so that no other block waits its full limit for work that will not come
+            ready = wait_count_or_abort(done, (unsigned)S, abort);
+            if (!ready) {
+                *(volatile unsigned*)abort = 1u;
+                *(volatile unsigned*)err = 3u;
+            }
+        }
+        if (__syncthreads_or(!ready)) return;
+        constexpr int LC = inblock_log_c(L1), TT = 1 << (L1 + LC - 4), G = kUnevenThreads / TT;
+        p.in = p.out;
+        p.log_s = L0;
+        p.swap_in = 0;
+        p.swap_out = b.inverse;
+        p.stw = b.stw1;
+        float2* sm = smem + (tid / TT) * (pass_smem_bytes(L1, LC, 2) / (int)sizeof(float2));
+        // pass 0 of this transform was written by other blocks: load through L2 only
+        pass_tile<L1, LC, 2, false, false, true>(p, (unsigned)((step - S) * G + tid / TT), 0, sm, tid % TT);
+    }
+}
+
+template <int M, int L0, int L1>
+__device__ __noinline__ void big_step_call(const BigItemArgs b, unsigned* done, unsigned* abort, unsigned* err, int step,
+                                           float2* smem, int tid) {
+    big_step<M, L0, L1>(b, done, abort, err, step, smem, tid);
+}
+
 // Any compiled split as a call, for the kernel that picks splits at run time. Inlining every
 // split into one kernel raised its spills at 64 registers from 164 to 536 bytes, even with three
 // identical splits; fixed kernels inline the one split they run.
@@ -134,6 +201,35 @@ __device__ __forceinline__ void big_choice(const UnevenArgs& a, const onefft_des
         case 1: big_item_call<M, kUnevenSplits[I][1][0], kUnevenSplits[I][1][1]>(b, smem, tid); break;
         case 2: big_item_call<M, kUnevenSplits[I][2][0], kUnevenSplits[I][2][1]>(b, smem, tid); break;
         default: big_item_call<M, kUnevenSplits[I][0][0], kUnevenSplits[I][0][1]>(b, smem, tid); break;
+        }
+    }
+}
+
+// One step of a 2^M transform (item `it`) with split CHOICE (or the batch's split, see big_choice).
+template <int M, int CHOICE>
+__device__ __forceinline__ void step_choice(const UnevenArgs& a, int it, const onefft_desc& d, int step, float2* smem,
+                                            int tid) {
+    constexpr int I = M - 13;
+    const BigItemArgs b{a.in + d.offset, a.out + d.offset, a.tw_lo[M], a.tw_hi[M],
+                        a.stw[M][0],     a.stw[M][1],      a.lo_bits[M], d.inverse};
+    unsigned* abort = a.done + a.nitems;
+    if constexpr (CHOICE != kSplitAtRunTime) {
+        big_step<M, kUnevenSplits[I][CHOICE][0], kUnevenSplits[I][CHOICE][1]>(b, a.done + it, abort, a.err, step, smem,
+                                                                             tid);
+    } else {
+        switch (a.split[M]) {
+        case 1:
+            big_step_call<M, kUnevenSplits[I][1][0], kUnevenSplits[I][1][1]>(b, a.done + it, abort, a.err, step, smem,
+                                                                           tid);
+            break;
+        case 2:
+            big_step_call<M, kUnevenSplits[I][2][0], kUnevenSplits[I][2][1]>(b, a.done + it, abort, a.err, step, smem,
+                                                                           tid);
+            break;
+        default:
+            big_step_call<M, kUnevenSplits[I][0][0], kUnevenSplits[I][0][1]>(b, a.done + it, abort, a.err, step, smem,
+                                                                           tid);
+            break;
         }
     }
 }
@@ -165,13 +261,32 @@ __global__ void __launch_bounds__(kUnevenThreads, 4) k_uneven(UnevenArgs a) {
     extern __shared__ float2 smem[];
     __shared__ int s_item;
     const int tid = threadIdx.x;
+    const int count = a.units ? a.nunits : a.nitems;
     for (;;) {
         if (tid == 0) s_item = atomicAdd(a.counter, 1);
         __syncthreads();
-        const int it = s_item;
+        const int s = s_item;
         __syncthreads();  // every thread has read s_item before it is overwritten
-        if (it >= a.nitems) break;
+        if (s >= count) break;
+        int it = s, step = -1;
+        if (a.units) {
+            const UnevenUnit u = a.units[s];
+            it = u.item;
+            step = u.step;
+        }
         const UnevenItem w = a.items[it];
+        if (step >= 0) {
+            const onefft_desc d = a.desc[w.first];
+            switch (w.log2n) {
+            case 13: step_choice<13, C13>(a, it, d, step, smem, tid); break;
+            case 14: step_choice<14, C14>(a, it, d, step, smem, tid); break;
+            case 15: step_choice<15, C15>(a, it, d, step, smem, tid); break;
+            case 16: step_choice<16, C16>(a, it, d, step, smem, tid); break;
+            default: break;
+            }
+            __syncthreads();  // the next unit may reuse shared memory
+            continue;
+        }
         switch (w.log2n) {
         case 0: tiny_item<0>(a, w, tid); break;
         case 1: tiny_item<1>(a, w, tid); break;

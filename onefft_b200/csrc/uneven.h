@@ -41,6 +41,20 @@ struct UnevenItem {
     int pad;
 };
 
+// One unit of the step-wise work queue: a small item whole (step < 0), or one step of 4096
+// values of a transform of 2^13 .. 2^16: steps 0 .. 2^(m-12) - 1 of its pass 0, then as many of
+// its pass 1.
+struct UnevenUnit {
+    int item;
+    int step;
+};
+
+// Pass-1 units of a transform follow the last pass-0 unit of that transform by at least this many
+// units in the queue: about the number of units the resident blocks run at once, so that pass
+// 1 rarely waits, while the values between the passes of the transforms in flight (this many
+// units of 32 KiB) stay far below the L2's 126 MB.
+constexpr int kUnevenLagUnits = 1024;
+
 // Kernel arguments, passed by value (about 1 KiB).
 struct UnevenArgs {
     const float2 *in;
@@ -49,6 +63,13 @@ struct UnevenArgs {
     const UnevenItem *items;
     int nitems;
     int *counter;  // work queue head, zeroed before every launch
+    // Step-wise queue (NULL: every block runs whole items, the transforms of 2^13 .. 2^16 tile
+    // after tile in one block): the units in queue order, and per item the pass-0 steps done,
+    // followed by one abort word (all zeroed before every launch, like the counter).
+    const UnevenUnit *units;
+    int nunits;
+    unsigned *done;
+    unsigned *err;  // set when a pass-1 unit's bounded wait for its pass 0 ran out
     const float2 *stw[kUnevenMaxLog2 + 1][2];  // stage tables: [m][0] single kernel / pass 0, [m][1] pass 1
     const double2 *tw_lo[kUnevenMaxLog2 + 1];
     const double2 *tw_hi[kUnevenMaxLog2 + 1];

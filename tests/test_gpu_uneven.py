@@ -70,6 +70,7 @@ def test_uneven_config3_full(ofb, oracle):
     d_out = T.full_like(d_in, float("nan"))
     batch.execute(d_in.data_ptr(), d_out.data_ptr())
     T.cuda.synchronize()
+    assert batch.status() == 0
     want = plain_path(ofb, T, log2n, inverse, offset, d_in)
     worst = compare(oracle, log2n, offset, d_out, want)
     print(f"uneven 20000: bitwise equal to the plain path except 2^13/2^14 (worst rel diff {worst:.3g})")
@@ -90,6 +91,7 @@ def test_uneven_config3_full(ofb, oracle):
     batch.execute(d_in.data_ptr(), d_out2.data_ptr())
     batch.execute(d_in.data_ptr(), d_out2.data_ptr())
     T.cuda.synchronize()
+    assert batch.status() == 0
     assert T.equal(d_out2, d_out)
     batch.destroy()
 
@@ -112,6 +114,7 @@ def test_uneven_all_sizes_and_gaps(ofb, oracle):
     d_out = T.full_like(d_in, sentinel)
     batch.execute(d_in.data_ptr(), d_out.data_ptr())
     T.cuda.synchronize()
+    assert batch.status() == 0
     want = plain_path(ofb, T, log2n, inverse, offset, d_in)
     compare(oracle, log2n, offset, d_out, want)
     covered = np.zeros(span, bool)
