@@ -342,20 +342,31 @@ def other_configs(torch, ofb, L, stream, peak):
                 "for bit except 2^13/2^14 (tests/test_gpu_uneven.py)"}
     ub.destroy()
     del x, y, groups
-    # split-BF16 tensor-core variant vs plain FP32 on the same batches
+    # split-BF16 tensor-core variants (3 and 6 product terms) vs plain FP32 on the same batches;
+    # "accepted" is the library's own decision (a plan that requires acceptance is built only at
+    # sizes where the variant met the FP32 error bound, measured by tests/test_gpu_bf16x3.py)
     for lg, batch in ((16, 256), (22, 16)):
         n = 1 << lg
         x = torch.randn(2 * n * batch, device="cuda", generator=g)
         y = torch.empty_like(x)
-        tc, fp = ofb.Plan(n, bf16x3=True), ofb.Plan(n)
-        t_tc = _time(torch, stream, lambda: tc.dev_forward(x.data_ptr(), y.data_ptr(), batch, sptr))
+        fp = ofb.Plan(n)
         t_fp = _time(torch, stream, lambda: fp.dev_forward(x.data_ptr(), y.data_ptr(), batch, sptr))
-        out[f"split-BF16 {batch} x 2^{lg}"] = {
-            "us_bf16x3": 1e6 * t_tc, "us_fp32": 1e6 * t_fp, "time_ratio_fp32_over_bf16x3": t_fp / t_tc,
-            "accepted": False,
-            "note": "rel RMS vs FP64 ~6.5e-6 against 1.5e-7 (FP32) on wide-range inputs: above the 2x bound, "
-                    "so no speedup at equal error exists (tests/test_gpu_bf16x3.py)"}
-        tc.destroy()
+        rec = {"us_fp32": 1e6 * t_fp}
+        for terms, kw in ((3, {"bf16x3": True}), (6, {"bf16x6": True})):
+            tc = ofb.Plan(n, **kw)
+            t_tc = _time(torch, stream, lambda: tc.dev_forward(x.data_ptr(), y.data_ptr(), batch, sptr))
+            tc.destroy()
+            try:
+                ofb.Plan(n, require_accepted=True, **kw).destroy()
+                accepted = True
+            except ValueError:
+                accepted = False
+            rec[f"us_bf16x{terms}"] = 1e6 * t_tc
+            rec[f"time_ratio_fp32_over_bf16x{terms}"] = t_fp / t_tc
+            rec[f"bf16x{terms}_accepted"] = accepted
+        rec["note"] = ("errors against FP64 per term count in tests/test_gpu_bf16x3.py; a speedup at equal error "
+                       "exists only where a variant is accepted and its time ratio exceeds 1")
+        out[f"split-BF16 {batch} x 2^{lg}"] = rec
         fp.destroy()
         del x, y
     # differentiable layer: forward + backward of sum |W * FFT(x)|^2, batch 512 x 8192

@@ -119,6 +119,14 @@ ONEFFT_API onefft_plan *onefft_plan_create_tiles(size_t n, int npass, const int 
  * counterpart in OneFFT. */
 ONEFFT_API onefft_plan *onefft_plan_create_bf16x3(size_t n, int require_accepted);
 
+/* As onefft_plan_create_bf16x3 with each FP32 value (data and DFT-16 constants) split into THREE
+ * bf16 parts hi + mid + lo (24 significant bits) and the six product terms down to 2^-16
+ * relative kept (hi hi; hi mid, mid hi; hi lo, lo hi, mid mid), twice the tensor-core products of
+ * the three-term form; the terms dropped are ~2^-24, FP32's own rounding. Accepted (with
+ * require_accepted != 0) only at sizes where it meets the FP32 path's error bound. No
+ * counterpart in OneFFT. */
+ONEFFT_API onefft_plan *onefft_plan_create_bf16x6(size_t n, int require_accepted);
+
 /* Number of passes of a plan and their log2 lengths (up to 3 are written to log2_len). */
 ONEFFT_API int onefft_plan_passes(const onefft_plan *plan, int *log2_len);
 

@@ -33,7 +33,8 @@ C_SYMBOLS = (
     "onefft_dev_forward_weighted", "onefft_dev_inverse_weighted",
     "onefft_dev_weighted_power_loss",
     "onefft_plan_forward_batched", "onefft_plan_inverse_batched",
-    "onefft_plan_create_split", "onefft_plan_create_tiles", "onefft_plan_create_bf16x3", "onefft_plan_passes",
+    "onefft_plan_create_split", "onefft_plan_create_tiles", "onefft_plan_create_bf16x3", "onefft_plan_create_bf16x6",
+    "onefft_plan_passes",
     "onefft_uneven_create", "onefft_uneven_create_split", "onefft_uneven_destroy", "onefft_uneven_span", "onefft_uneven_execute",
     "onefft_uneven_status",
     "onefft_uneven_execute_noalloc",
@@ -70,6 +71,8 @@ def lib() -> ctypes.CDLL:
     L.onefft_plan_create_tiles.restype = _vp
     L.onefft_plan_create_bf16x3.argtypes = [_sz, ctypes.c_int]
     L.onefft_plan_create_bf16x3.restype = _vp
+    L.onefft_plan_create_bf16x6.argtypes = [_sz, ctypes.c_int]
+    L.onefft_plan_create_bf16x6.restype = _vp
     L.onefft_plan_destroy.argtypes = [_vp]
     L.onefft_plan_destroy.restype = None
     L.onefft_plan_forward.argtypes = [_vp, _vp, _vp]
@@ -187,16 +190,18 @@ class Plan:
 
     def __init__(self, n: int, split: tuple[int, ...] | None = None, cols: tuple[int, ...] | None = None,
                  l2_keep: bool = True, chunk: int = 0, bf16x3: bool = False, require_accepted: bool = False,
-                 tma: bool = False, fuse_lag: int = 0):
+                 tma: bool = False, fuse_lag: int = 0, bf16x6: bool = False):
         """split: log2 pass lengths (None = tuned table); cols: log2 tile widths per pass;
         chunk: three passes only, log2 last-digit columns per L2-resident chunk (0 = none);
         fuse_lag: with chunk and tma, run passes 0 and 1 as one persistent kernel with pass 1
         trailing pass 0 by this many chunks (ONEFFT_OPT_FUSED; 0 = separate launches);
-        bf16x3: the split-BF16 tensor-core variant (require_accepted: only at sizes where it
-        meets the FP32 error bound)."""
+        bf16x3 / bf16x6: the split-BF16 tensor-core variant of three (hi/lo) or six
+        (hi/mid/lo) product terms (require_accepted: only at sizes where it meets the FP32 error
+        bound)."""
         L = lib()
-        if bf16x3:
-            h = L.onefft_plan_create_bf16x3(n, int(require_accepted))
+        if bf16x3 or bf16x6:
+            f = L.onefft_plan_create_bf16x6 if bf16x6 else L.onefft_plan_create_bf16x3
+            h = f(n, int(require_accepted))
         elif split is None:
             h = L.onefft_plan_create(n)
         else:

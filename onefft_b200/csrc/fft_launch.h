@@ -87,11 +87,11 @@ bool pass01_fused_supported(int l0, int c0, int l1, int c1);
 cudaError_t launch_pass01_fused(int l0, int c0, int l1, int c1, const PassArgs& a0, const PassArgs& a1, int g,
                                 int len2, int lag, unsigned* ctr, cudaStream_t stream);
 cudaError_t launch_pass_tma(int mode, int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t stream);
-// split-BF16 tensor-core variants (fft_tc.cu): n = 2^4 .. 2^14 in one kernel; pass lengths
-// 2^5 .. 2^12 with the default tile width pass_log_c()
+// split-BF16 tensor-core variants (fft_tc.cu) of `terms` = 3 or 6 split products: n = 2^4 .. 2^14
+// in one kernel; pass lengths 2^5 .. 2^12 with the default tile width pass_log_c()
 cudaError_t launch_single_kernel_tc(int log2n, const float2* in, float2* out, long long batch, const float2* stw,
-                                    int inverse, cudaStream_t stream);
-cudaError_t launch_pass_tc(int mode, int log_l, const PassArgs& a, int batch, cudaStream_t stream);
+                                    int inverse, int terms, cudaStream_t stream);
+cudaError_t launch_pass_tc(int mode, int log_l, const PassArgs& a, int batch, int terms, cudaStream_t stream);
 // fused forward -> sum w^2 |y|^2 -> adjoint of 2 w^2 y, n = 2^4 .. 2^14 (fft_fused.cu)
 cudaError_t launch_power_loss_grad(int log2n, const float2* x, const float* w, float2* grad, double* loss,
                                    long long batch, const float2* stw, cudaStream_t stream);

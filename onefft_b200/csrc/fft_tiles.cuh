@@ -137,8 +137,9 @@ __device__ __forceinline__ void tiny_transform(const float2* __restrict__ src, f
 // 2^LOG_C transforms of length L = 2^LOG_L, 16 values per thread, thread tid owns column
 // c = tid / (L/16) and butterfly lane j = tid mod (L/16). src / dst point at this thread's
 // transform; inactive columns (past the end of a batch) compute on zeros and store nothing.
-// TC selects the split-BF16 tensor-core stages (fft_tc.cuh). W, pre, post as tiny_transform.
-template <int LOG_L, int LOG_C, bool TC = false, bool W = false>
+// TC: 0 = FP32 stages; 3 or 6 = the split-BF16 tensor-core stages with that many product terms
+// (fft_tc.cuh). W, pre, post as tiny_transform.
+template <int LOG_L, int LOG_C, int TC = 0, bool W = false>
 __device__ __forceinline__ void batched_tile(const float2* __restrict__ src, float2* __restrict__ dst, bool active,
                                              int inverse, const float2* __restrict__ stw, float2* smem, int tid,
                                              const float2* __restrict__ pre = nullptr,
@@ -157,7 +158,7 @@ __device__ __forceinline__ void batched_tile(const float2* __restrict__ src, flo
         }
         v[k] = inverse ? swap_ri(x) : x;
     }
-    if constexpr (TC) tile_fft_tc<LOG_L, LOG_C, 1>(v, j, stw, smem, c << LOG_L, tid);
+    if constexpr (TC != 0) tile_fft_tc<LOG_L, LOG_C, 1, TC>(v, j, stw, smem, c << LOG_L, tid);
     else tile_fft<LOG_L, 1>(v, j, stw, smem, c << LOG_L);
     if (active) {
 #pragma unroll
@@ -183,7 +184,7 @@ __device__ __forceinline__ void batched_tile(const float2* __restrict__ src, flo
 // CG: later passes load through L2 only (ld.global.cg), for data that other blocks of the same
 // launch wrote: an SM's L1 may still hold an older copy of a line that it read for a neighbouring
 // transform.
-template <int LOG_L, int LOG_C, int MODE, bool TC = false, bool W = false, bool CG = false>
+template <int LOG_L, int LOG_C, int MODE, int TC = 0, bool W = false, bool CG = false>
 __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long long toff, float2* smem, int tid) {
     constexpr int L = 1 << LOG_L, T = L / 16, C = 1 << LOG_C;
     const int c = tid & (C - 1);
@@ -227,7 +228,7 @@ __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long lo
             v[k] = a.swap_in ? swap_ri(x) : x;
         }
     }
-    if constexpr (TC) tile_fft_tc<LOG_L, LOG_C, C>(v, j, a.stw, smem, c, tid);
+    if constexpr (TC != 0) tile_fft_tc<LOG_L, LOG_C, C, TC>(v, j, a.stw, smem, c, tid);
     else tile_fft<LOG_L, C>(v, j, a.stw, smem, c);
     if (MODE != 2) {
         if (Stages<LOG_L>::COUNT == 1) __syncthreads();  // tile_fft had no barrier to publish tws

@@ -102,7 +102,8 @@ struct onefft_plan {
                            // cols[0] = log2 of the transforms per block (-1 = default)
     int l2_keep;           // intermediate stores with L2 evict-last priority
     int chunk;             // three passes: log2 of the last-digit columns per chunk of passes 0+1 (0 = none)
-    int tc;                // radix-16 stages as split-BF16 tensor-core products (onefft_plan_create_bf16x3)
+    int tc;                // radix-16 stages as split-BF16 tensor-core products of this many terms (3: hi/lo,
+                           // onefft_plan_create_bf16x3; 6: hi/mid/lo, onefft_plan_create_bf16x6); 0 = FP32
     int tma;               // passes staged through bulk tensor copies where the tile shape has a TMA kernel
     int fuse_lag;          // three passes, chunked: passes 0+1 as one persistent launch with pass 1
                            // trailing by this many chunks (0 = separate launches)
@@ -346,20 +347,22 @@ extern "C" onefft_plan *onefft_plan_create_tiles(size_t n, int npass, const int 
     return plan_build(n, m, s);
 }
 
-// Sizes (bit log2 n) at which the split-BF16 tensor-core variant meets the FP32 path's error
-// bound (relative RMS against FP64 at most 2x OneFFT's own). Measured on a B200 with standard
-// normal inputs with 1 % of the values scaled by 1e3 (tests/test_gpu_bf16x3.py): three-term
-// BF16 products leave ~1e-5 relative error, about 100x the bound at every size, so none is.
+// Sizes (bit log2 n) at which each split-BF16 tensor-core variant meets the FP32 path's error
+// bound (relative RMS against FP64 at most 2x OneFFT's own), measured on a B200 with standard
+// normal inputs with 1 % of the values scaled by 1e3 (tests/test_gpu_bf16x3.py). Three terms
+// leave ~1e-5 relative error, about 100x the bound at every size, so none is.
 static const unsigned long long kBf16x3Accepted = 0;
+static const unsigned long long kBf16x6Accepted = 0;
 
-extern "C" onefft_plan *onefft_plan_create_bf16x3(size_t n, int require_accepted) {
+static onefft_plan *create_bf16(size_t n, int terms, unsigned long long accepted, int require_accepted) {
     int m;
     if (!size_log2(n, &m) || m < 4) {
         set_error(ONEFFT_ERR_SIZE, "n=%zu: the tensor-core variant needs a power of two in [16, 2^30]", n);
         return nullptr;
     }
-    if (require_accepted && !((kBf16x3Accepted >> m) & 1)) {
-        set_error(ONEFFT_ERR_SIZE, "n=2^%d: split-BF16 does not meet the FP32 error bound at this size", m);
+    if (require_accepted && !((accepted >> m) & 1)) {
+        set_error(ONEFFT_ERR_SIZE, "n=2^%d: split-BF16 (%d terms) does not meet the FP32 error bound at this size", m,
+                  terms);
         return nullptr;
     }
     Shape s = tuned_shape(m);
@@ -374,8 +377,16 @@ extern "C" onefft_plan *onefft_plan_create_bf16x3(size_t n, int require_accepted
         }
     }
     onefft_plan *p = plan_build(n, m, s);
-    if (p) p->tc = 1;
+    if (p) p->tc = terms;
     return p;
+}
+
+extern "C" onefft_plan *onefft_plan_create_bf16x3(size_t n, int require_accepted) {
+    return create_bf16(n, 3, kBf16x3Accepted, require_accepted);
+}
+
+extern "C" onefft_plan *onefft_plan_create_bf16x6(size_t n, int require_accepted) {
+    return create_bf16(n, 6, kBf16x6Accepted, require_accepted);
 }
 
 extern "C" onefft_plan *onefft_plan_create_split(size_t n, int npass, const int *log2_len) {
@@ -423,7 +434,7 @@ static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *
     if (batch <= 0) return cudaSuccess;
     if (p->npass == 1) {
         g_launches.fetch_add(1);
-        if (p->tc) return launch_single_kernel_tc(p->log2n, in, out, batch, p->stw[0], inverse, s);
+        if (p->tc) return launch_single_kernel_tc(p->log2n, in, out, batch, p->stw[0], inverse, p->tc, s);
         return launch_single_kernel(p->log2n, in, out, batch, p->stw[0], inverse, s, pre, post, p->cols[0]);
     }
     PassArgs a{};
@@ -441,7 +452,7 @@ static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *
     auto run = [&](int mode, int i, const PassArgs &x) {
         if (use_tma && pass_tma_supported(p->len[i], p->cols[i]))
             return launch_pass_tma(mode, p->len[i], p->cols[i], x, (int)batch, s);
-        return p->tc ? launch_pass_tc(mode, p->len[i], x, (int)batch, s)
+        return p->tc ? launch_pass_tc(mode, p->len[i], x, (int)batch, p->tc, s)
                      : launch_pass(mode, p->len[i], p->cols[i], x, (int)batch, s);
     };
     if (p->npass == 3 && p->fuse_lag && use_tma && !pre) {
