@@ -6,6 +6,8 @@
     python -m onefft_b200.profile_case --uneven 2000                      # the uneven-batch kernel
     python -m onefft_b200.profile_case --log2n 13 --batch 512 --loss      # fused loss + gradient
     python -m onefft_b200.profile_case --log2n 16 --batch 256 --bf16x3    # split-BF16 tensor cores
+    python -m onefft_b200.profile_case --log2n 24 --split 8,8,8 --cols 4,4,4 --tma --chunk 4 --fuse-lag 1
+                                                                          # fused passes 0+1
 
 Inputs are seeded standard-normal values on the device; the plan (and its table kernels) is
 built before the timed transforms, so `ncu -k regex:k_pass -s <n>` can skip to them.
@@ -31,7 +33,10 @@ def main():
     ap.add_argument("--chunk", type=int, default=0, help="three passes: log2 last-digit columns per chunk")
     ap.add_argument("--tma", action="store_true", help="with --split: TMA-staged passes")
     ap.add_argument("--loss", action="store_true", help="the fused weighted-power loss and gradient")
-    ap.add_argument("--bf16x3", action="store_true", help="the split-BF16 tensor-core plan")
+    ap.add_argument("--bf16x3", action="store_true", help="the split-BF16 tensor-core plan (three terms)")
+    ap.add_argument("--bf16x6", action="store_true", help="the split-BF16 tensor-core plan (six terms)")
+    ap.add_argument("--fuse-lag", type=int, default=0, help="with --chunk and --tma: fused passes 0+1")
+    ap.add_argument("--no-l2-keep", action="store_true", help="with --split: no L2 eviction hints")
     ap.add_argument("--uneven", type=int, default=0, help="run an uneven batch of this many transforms")
     args = ap.parse_args()
     g = torch.Generator(device="cuda").manual_seed(7)
@@ -51,7 +56,11 @@ def main():
     n = 1 << args.log2n
     split = tuple(int(v) for v in args.split.split(",")) if args.split else None
     cols = tuple(int(v) for v in args.cols.split(",")) if args.cols else None
-    plan = ofb.Plan(n, bf16x3=True) if args.bf16x3 else ofb.Plan(n, split=split, cols=cols, chunk=args.chunk, tma=args.tma)
+    if args.bf16x3 or args.bf16x6:
+        plan = ofb.Plan(n, bf16x3=args.bf16x3, bf16x6=args.bf16x6)
+    else:
+        plan = ofb.Plan(n, split=split, cols=cols, chunk=args.chunk, tma=args.tma, fuse_lag=args.fuse_lag,
+                        l2_keep=not args.no_l2_keep)
     if args.loss:
         x = torch.randn(2 * n * args.batch, device="cuda", generator=g)
         w = torch.rand(n, device="cuda", generator=g)
