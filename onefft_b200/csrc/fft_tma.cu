@@ -157,11 +157,16 @@ __host__ __device__ constexpr int tma_smem_bytes(int log_l, int log_c) {
 // the same in every thread, if the copy's bounded wait expired: the tile then recorded the
 // failure in the plan's error word, let the copy land and wrote nothing.
 // W: the first pass multiplies its input by a.pre, the last pass its output by a.post
-// (instantiated only for weighted calls).
-template <int LOG_L, int LOG_C, int MODE, bool W>
+// (instantiated only for weighted calls). after_wait() runs in every thread once the copy has
+// landed, before the tile's arithmetic (the fused kernel publishes its previous tile there).
+struct NoHook {
+    __device__ void operator()() const {}
+};
+
+template <int LOG_L, int LOG_C, int MODE, bool W, class Hook = NoHook>
 __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* tin, const CUtensorMap* tout,
                                          unsigned t, int b, float2* smem, uint64_t* bar, unsigned parity, bool fresh,
-                                         int tid) {
+                                         int tid, Hook after_wait = Hook()) {
     constexpr int L = 1 << LOG_L, T = L / 16, C = 1 << LOG_C;
     const int c = tid & (C - 1);
     const int j = tid >> LOG_C;
@@ -201,6 +206,7 @@ __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* t
         }
         return false;
     }
+    after_wait();
     float2 v[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
@@ -348,6 +354,19 @@ __global__ void __launch_bounds__(1 << (L0 + C0 - 4), (fused_min_blocks<L0, C0, 
         __syncthreads();
         unsigned s = *shared_word, parity = 0;
         bool fresh = true;
+        // A pass-0 tile is counted as done (fence, then the chunk's counter) only once the block's
+        // next tile copy has landed: by then its stores have long reached L2 and the fence costs
+        // little, where fencing right after the stores held the block for their whole round
+        // trip. `pending` is that tile's chunk (-1: none); it is published before any wait on a
+        // counter, so no block ever waits for a count that it holds itself.
+        int pending = -1;
+        auto publish = [&]() {
+            if (pending >= 0 && tid == 0) {
+                __threadfence();  // the tile's stores (all threads, ordered by the barriers since)
+                atomicAdd(f.ctr + 2 + pending, 1u);
+            }
+            pending = -1;
+        };
         while (s < f.total) {
             int pass;
             unsigned chunk, tile;
@@ -358,13 +377,10 @@ __global__ void __launch_bounds__(1 << (L0 + C0 - 4), (fused_min_blocks<L0, C0, 
             if (pass == 0) {
                 PassArgs a = f.p0;
                 a.inner_base = chunk << f.g;
-                ok = tma_tile<L0, C0, 0, false>(a, &tin, &tin, tile, 0, smem, bar, parity, fresh, tid);
-                __syncthreads();  // every thread's stores of the tile are issued
-                if (ok && tid == 0) {
-                    __threadfence();  // ... and visible at GPU scope before the count says so
-                    atomicAdd(f.ctr + 2 + chunk, 1u);
-                }
+                ok = tma_tile<L0, C0, 0, false>(a, &tin, &tin, tile, 0, smem, bar, parity, fresh, tid, publish);
+                if (ok) pending = (int)chunk;
             } else {
+                publish();
                 bool ready = true;
                 if (tid == 0) {
                     ready = !g_expire_waits && wait_count(f.ctr + 2 + chunk, f.t0);
@@ -383,9 +399,10 @@ __global__ void __launch_bounds__(1 << (L0 + C0 - 4), (fused_min_blocks<L0, C0, 
             if (!ok) break;  // block-uniform: an expired wait, recorded in the error word
             parity ^= 1u;
             fresh = false;
-            __syncthreads();  // the next-tile word is written; the tile's shared memory is free
+            __syncthreads();  // the next-tile word is written; the tile's stores are issued
             s = *shared_word;
         }
+        publish();  // the last pass-0 tile (after the barrier above, or after a failed tile)
     }
     // The last block to leave zeroes the counters for the next launch on this slot: every other
     // block has left its loop, so none touches them again.
