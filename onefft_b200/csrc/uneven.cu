@@ -262,12 +262,15 @@ __global__ void __launch_bounds__(kUnevenThreads, 4) k_uneven(UnevenArgs a) {
     __shared__ int s_item;
     const int tid = threadIdx.x;
     const int count = a.units ? a.nunits : a.nitems;
-    for (;;) {
-        if (tid == 0) s_item = atomicAdd(a.counter, 1);
-        __syncthreads();
-        const int s = s_item;
+    if (tid == 0) s_item = atomicAdd(a.counter, 1);
+    __syncthreads();
+    int s = s_item;
+    for (;; s = s_item) {
         __syncthreads();  // every thread has read s_item before it is overwritten
         if (s >= count) break;
+        // the next unit's index, fetched while this one runs (its round trip to L2 would
+        // otherwise hold the whole block between units)
+        if (tid == 0) s_item = atomicAdd(a.counter, 1);
         int it = s, step = -1;
         if (a.units) {
             const UnevenUnit u = a.units[s];
