@@ -157,16 +157,24 @@ __host__ __device__ constexpr int tma_smem_bytes(int log_l, int log_c) {
 // the same in every thread, if the copy's bounded wait expired: the tile then recorded the
 // failure in the plan's error word, let the copy land and wrote nothing.
 // W: the first pass multiplies its input by a.pre, the last pass its output by a.post
-// (instantiated only for weighted calls). after_wait() runs in every thread once the copy has
-// landed, before the tile's arithmetic (the fused kernel publishes its previous tile there).
+// (instantiated only for weighted calls).
+// Hooks, for the persistent fused kernel: thread 0 calls ready() before issuing the copy (false:
+// the tile is not run and tma_tile returns false), and issued() right after issuing it, so that
+// work which waits on memory overlaps the copy; every thread calls landed() once the copy has
+// landed, before the tile's arithmetic.
 struct NoHook {
     __device__ void operator()() const {}
 };
+struct AlwaysReady {
+    __device__ bool operator()() const { return true; }
+};
 
-template <int LOG_L, int LOG_C, int MODE, bool W, class Hook = NoHook>
+template <int LOG_L, int LOG_C, int MODE, bool W, class Ready = AlwaysReady, class Issued = NoHook,
+          class Landed = NoHook>
 __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* tin, const CUtensorMap* tout,
                                          unsigned t, int b, float2* smem, uint64_t* bar, unsigned parity, bool fresh,
-                                         int tid, Hook after_wait = Hook()) {
+                                         int tid, Ready ready = Ready(), Issued issued = Issued(),
+                                         Landed landed = Landed()) {
     constexpr int L = 1 << LOG_L, T = L / 16, C = 1 << LOG_C;
     const int c = tid & (C - 1);
     const int j = tid >> LOG_C;
@@ -174,20 +182,25 @@ __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* t
                                       : ((a.outer_base + (t >> a.tli)) << a.outer_shift) + a.inner_base +
                                             ((t & ((1u << a.tli) - 1)) << LOG_C);
     const int q0 = (int)(col0 & ((1u << a.log_s) - 1)), h = (int)(col0 >> a.log_s);
+    bool go = true;
     if (tid == 0) {
         if (fresh) mbar_init(bar, 1);
         else asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(bar, (unsigned)(C * L * sizeof(float2)));
-        // With l2_keep the array between passes should stay in L2: the input (read once) and
-        // the last pass's tile (read for the last time) are loaded evict-first.
-        if (a.l2_keep && MODE != 1) {
-            const unsigned long long first = policy_evict_first();
-            if (MODE == 0) tma_load_4d_hint(smem, tin, (int)col0, 0, 0, b, bar, first);
-            else tma_load_5d_hint(smem, tin, q0, 0, 0, h, b, bar, first);
-        } else if (MODE == 0) {
-            tma_load_4d(smem, tin, (int)col0, 0, 0, b, bar);
-        } else {
-            tma_load_5d(smem, tin, q0, 0, 0, h, b, bar);
+        go = ready();
+        if (go) {
+            mbar_expect_tx(bar, (unsigned)(C * L * sizeof(float2)));
+            // With l2_keep the array between passes should stay in L2: the input (read once)
+            // and the last pass's tile (read for the last time) are loaded evict-first.
+            if (a.l2_keep && MODE != 1) {
+                const unsigned long long first = policy_evict_first();
+                if (MODE == 0) tma_load_4d_hint(smem, tin, (int)col0, 0, 0, b, bar, first);
+                else tma_load_5d_hint(smem, tin, q0, 0, 0, h, b, bar, first);
+            } else if (MODE == 0) {
+                tma_load_4d(smem, tin, (int)col0, 0, 0, b, bar);
+            } else {
+                tma_load_5d(smem, tin, q0, 0, 0, h, b, bar);
+            }
+            issued();
         }
     }
     // inter-pass twiddle factors (as pass_tile) while the copy is in flight
@@ -197,7 +210,8 @@ __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* t
         pass_twiddle_rows<LOG_L, LOG_C, MODE>(a, col0, tws, tid, C * T);
         wjf = pass_twiddle_lane<LOG_L>(a, MODE == 0 ? col0 + c : (col0 >> a.log_s) << a.log_s, j);
     }
-    __syncthreads();  // the barrier is initialised (and armed) before anyone waits on it
+    // the barrier is initialised (and armed) before anyone waits on it
+    if (__syncthreads_or(!go)) return false;  // nothing was issued: nothing to wait for
     const bool ok = !g_expire_waits && mbar_wait(bar, parity);
     if (__syncthreads_or(!ok)) {
         if (tid == 0) {
@@ -206,7 +220,7 @@ __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* t
         }
         return false;
     }
-    after_wait();
+    landed();
     float2 v[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
@@ -345,14 +359,17 @@ __global__ void __launch_bounds__(1 << (L0 + C0 - 4), (fused_min_blocks<L0, C0, 
                                                                         : tma_bar_offset(L1, C1);
     extern __shared__ __align__(1024) float2 smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + BAR);
-    unsigned* shared_word = reinterpret_cast<unsigned*>(smem + BAR + 1);  // the next tile, then "last block"
+    // two words after the mbarrier: the next tile's index, alternating by iteration (written by
+    // thread 0 while the current tile's copy is in flight, read by all after the tile), then the
+    // "last block" flag
+    unsigned* shared_word = reinterpret_cast<unsigned*>(smem + BAR + 1);
     const int tid = threadIdx.x;
     if (smem_u32(smem) & 127) {  // bulk tensor copies need a 128-byte aligned destination
         if (tid == 0) *(volatile unsigned*)f.p0.err = 2u;
     } else {
-        if (tid == 0) *shared_word = atomicAdd(f.ctr, 1u);
+        if (tid == 0) shared_word[0] = atomicAdd(f.ctr, 1u);
         __syncthreads();
-        unsigned s = *shared_word, parity = 0;
+        unsigned s = shared_word[0], parity = 0, iter = 0;
         bool fresh = true;
         // A pass-0 tile is counted as done (fence, then the chunk's counter) only once the block's
         // next tile copy has landed: by then its stores have long reached L2 and the fence costs
@@ -371,36 +388,38 @@ __global__ void __launch_bounds__(1 << (L0 + C0 - 4), (fused_min_blocks<L0, C0, 
             int pass;
             unsigned chunk, tile;
             fused_decode(f, s, pass, chunk, tile);
-            __syncthreads();  // every thread has read the next-tile word
-            if (tid == 0) *shared_word = atomicAdd(f.ctr, 1u);  // fetched while this tile runs
+            unsigned* next = shared_word + ((iter + 1) & 1);  // read by all only after this tile
+            auto fetch_next = [&]() { *next = atomicAdd(f.ctr, 1u); };  // thread 0, copy in flight
             bool ok;
             if (pass == 0) {
                 PassArgs a = f.p0;
                 a.inner_base = chunk << f.g;
-                ok = tma_tile<L0, C0, 0, false>(a, &tin, &tin, tile, 0, smem, bar, parity, fresh, tid, publish);
+                ok = tma_tile<L0, C0, 0, false>(a, &tin, &tin, tile, 0, smem, bar, parity, fresh, tid, AlwaysReady(),
+                                                fetch_next, publish);
                 if (ok) pending = (int)chunk;
             } else {
                 publish();
-                bool ready = true;
-                if (tid == 0) {
-                    ready = !g_expire_waits && wait_count(f.ctr + 2 + chunk, f.t0);
+                // thread 0: wait until every pass-0 tile of the chunk is published, then issue
+                // the copy; the other threads compute the tile's twiddle factors meanwhile
+                auto chunk_ready = [&]() {
+                    const bool r = !g_expire_waits && wait_count(f.ctr + 2 + chunk, f.t0);
                     // the chunk's values were written by other blocks through the generic proxy;
                     // this block reads them with a bulk tensor copy (the async proxy)
                     asm volatile("fence.proxy.async.global;" ::: "memory");
-                    if (!ready) *(volatile unsigned*)f.p1.err = 3u;
-                }
-                ok = !__syncthreads_or(!ready);
-                if (ok) {
-                    PassArgs a = f.p1;
-                    a.outer_base = chunk << f.g;
-                    ok = tma_tile<L1, C1, 1, false>(a, &tmid, &tmid, tile, 0, smem, bar, parity, fresh, tid);
-                }
+                    if (!r) *(volatile unsigned*)f.p1.err = 3u;
+                    return r;
+                };
+                PassArgs a = f.p1;
+                a.outer_base = chunk << f.g;
+                ok = tma_tile<L1, C1, 1, false>(a, &tmid, &tmid, tile, 0, smem, bar, parity, fresh, tid, chunk_ready,
+                                                fetch_next);
             }
             if (!ok) break;  // block-uniform: an expired wait, recorded in the error word
             parity ^= 1u;
             fresh = false;
             __syncthreads();  // the next-tile word is written; the tile's stores are issued
-            s = *shared_word;
+            s = *next;
+            ++iter;
         }
         publish();  // the last pass-0 tile (after the barrier above, or after a failed tile)
     }
