@@ -346,9 +346,11 @@ __device__ __forceinline__ void fused_decode(const FusedArgs& f, unsigned s, int
 }
 
 // Both tile shapes run with the same number of threads: 2^(L0 + C0 - 4) = 2^(L1 + C1 - 4).
+// Blocks per SM the register allocation must allow: as many as the separate pass kernels of the
+// same tiles get (the fused kernels are latency-bound tile machines, so residency matters).
 template <int L0, int C0, int L1, int C1>
 constexpr int fused_min_blocks() {
-    return L0 == 8 && C0 == 4 && L1 == 9 && C1 == 3 ? 5 : 0;
+    return L0 + C0 == 11 ? 8 : L0 + C0 == 12 ? 5 : L0 + C0 == 13 ? 2 : 0;
 }
 
 template <int L0, int C0, int L1, int C1>
