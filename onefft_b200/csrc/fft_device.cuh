@@ -182,9 +182,8 @@ __host__ __device__ constexpr int stage_table_entries(int log_l) {
 
 // Compute stage s in registers: twiddle the inputs (s > 0), run 16/R butterflies of radix R.
 // Butterfly i of this thread has b = j + T i and inputs v[i + (16/R) q]; its output p is left in
-// v[i + (16/R) p]. SHARED_TW: stw points at a copy of the stage table in shared memory (read
-// with plain loads) instead of the plan's table in global memory (read-only cache).
-template <int LOG_L, int S, bool SHARED_TW = false>
+// v[i + (16/R) p].
+template <int LOG_L, int S>
 __device__ __forceinline__ void stage_compute(float2 (&v)[16], int j, const float2* __restrict__ stw) {
     using St = Stages<LOG_L>;
     constexpr int LR = St::log2_radix(S);
@@ -200,7 +199,7 @@ __device__ __forceinline__ void stage_compute(float2 (&v)[16], int j, const floa
             const int r = (j + St::T * i) & (NS - 1);
             const float2* tw = stw + St::tw_offset(S) + r;
 #pragma unroll
-            for (int q = 1; q < R; ++q) a[q] = cmul(a[q], SHARED_TW ? tw[(q - 1) * NS] : __ldg(tw + (q - 1) * NS));
+            for (int q = 1; q < R; ++q) a[q] = cmul(a[q], __ldg(tw + (q - 1) * NS));
         }
         dft<R>(a);
 #pragma unroll
@@ -230,11 +229,11 @@ __host__ __device__ constexpr int padc(int d) { return d + (d >> 4); }
 // The column's element e lives at linear tile index e * LM + cofs: LM = C, cofs = c for the
 // column-interleaved layout ([e][c], C columns), LM = 1, cofs = c L for whole columns ([c][e]).
 // All threads of the block must call this (it synchronises).
-template <int LOG_L, int LM, int S = 0, bool SHARED_TW = false>
+template <int LOG_L, int LM, int S = 0>
 __device__ __forceinline__ void tile_fft(float2 (&v)[16], int j, const float2* __restrict__ stw, float2* smem,
                                          int cofs) {
     using St = Stages<LOG_L>;
-    stage_compute<LOG_L, S, SHARED_TW>(v, j, stw);
+    stage_compute<LOG_L, S>(v, j, stw);
     if constexpr (S + 1 < St::COUNT) {
         // intermediate stages are radix 16: one butterfly per thread, b = j, output p at
         // E0 + p Ns with E0 = (j / Ns) 16 Ns + (j mod Ns)
@@ -248,7 +247,7 @@ __device__ __forceinline__ void tile_fft(float2 (&v)[16], int j, const float2* _
 #pragma unroll
         for (int k = 0; k < 16; ++k) v[k] = r[padc(k * St::T * LM)];
         __syncthreads();
-        tile_fft<LOG_L, LM, S + 1, SHARED_TW>(v, j, stw, smem, cofs);
+        tile_fft<LOG_L, LM, S + 1>(v, j, stw, smem, cofs);
     }
 }
 

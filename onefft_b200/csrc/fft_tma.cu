@@ -145,13 +145,8 @@ constexpr int tma_min_blocks() {
 __host__ __device__ constexpr int tma_bar_offset(int log_l, int log_c) {
     return (1 << (log_l + log_c)) + (1 << (log_l + log_c - 4)) + 17 * (1 << log_c);
 }
-// Tiles of up to 1024 values per column copy their stage twiddle table (at most 1008 entries, 8
-// KB) into shared memory while the tile's copy is in flight, behind the mbarrier and two spare
-// words, so the radix stages read it there rather than through L1 and L2 (longer tiles keep the
-// read-only cache: their tables of 16 and 32 KB would cost blocks per SM).
-__host__ __device__ constexpr int tma_shared_tw(int log_l) { return log_l <= 10 ? stage_table_entries(log_l) : 0; }
 __host__ __device__ constexpr int tma_smem_bytes(int log_l, int log_c) {
-    return (int)sizeof(float2) * (tma_bar_offset(log_l, log_c) + 2 + tma_shared_tw(log_l)) + 16;
+    return (int)sizeof(float2) * (tma_bar_offset(log_l, log_c) + 2) + 16;
 }
 
 // One tile of a pass, MODE as k_pass, run by all threads of the block: the tile arrives through
@@ -177,11 +172,10 @@ struct AlwaysReady {
 template <int LOG_L, int LOG_C, int MODE, bool W, class Ready = AlwaysReady, class Issued = NoHook,
           class Landed = NoHook>
 __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* tin, const CUtensorMap* tout,
-                                         unsigned t, int b, float2* smem, uint64_t* bar, float2* stage_tw,
-                                         unsigned parity, bool fresh, int tid, Ready ready = Ready(),
-                                         Issued issued = Issued(), Landed landed = Landed()) {
+                                         unsigned t, int b, float2* smem, uint64_t* bar, unsigned parity, bool fresh,
+                                         int tid, Ready ready = Ready(), Issued issued = Issued(),
+                                         Landed landed = Landed()) {
     constexpr int L = 1 << LOG_L, T = L / 16, C = 1 << LOG_C;
-    constexpr int SHARED_TW = tma_shared_tw(LOG_L);
     const int c = tid & (C - 1);
     const int j = tid >> LOG_C;
     const unsigned col0 = a.tli >= 31 ? (t << LOG_C)
@@ -209,10 +203,7 @@ __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* t
             issued();
         }
     }
-    // the stage table (see tma_shared_tw) and the inter-pass twiddle factors (as pass_tile)
-    // while the copy is in flight
-    if constexpr (SHARED_TW > 0)
-        for (int i = tid; i < SHARED_TW; i += C * T) stage_tw[i] = __ldg(a.stw + i);
+    // inter-pass twiddle factors (as pass_tile) while the copy is in flight
     float2* tws = smem + spad(C * L - 1) + 1;
     float2 wjf = make_float2(1.f, 0.f);
     if (MODE != 2) {
@@ -241,7 +232,7 @@ __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* t
         v[k] = a.swap_in ? swap_ri(x) : x;
     }
     __syncthreads();  // the dense tile is consumed; the exchanges reuse its memory
-    tile_fft<LOG_L, C, 0, (SHARED_TW > 0)>(v, j, SHARED_TW > 0 ? stage_tw : a.stw, smem, c);
+    tile_fft<LOG_L, C>(v, j, a.stw, smem, c);
     if (MODE != 2) {
         if (Stages<LOG_L>::COUNT == 1) __syncthreads();
         const float2* tw = tws + (MODE == 0 ? c * 17 : 0);
@@ -302,8 +293,8 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_
         if (threadIdx.x == 0) *(volatile unsigned*)a.err = 2u;
         return;
     }
-    tma_tile<LOG_L, LOG_C, MODE, W>(a, &tin, &tout, blockIdx.x, (int)blockIdx.y, smem, bar,
-                                    smem + tma_bar_offset(LOG_L, LOG_C) + 2, 0u, true, (int)threadIdx.x);
+    tma_tile<LOG_L, LOG_C, MODE, W>(a, &tin, &tout, blockIdx.x, (int)blockIdx.y, smem, bar, 0u, true,
+                                    (int)threadIdx.x);
 }
 
 // ---- passes 0 and 1 of a three-pass transform in one persistent launch -----------------------
@@ -374,7 +365,6 @@ __global__ void __launch_bounds__(1 << (L0 + C0 - 4), (fused_min_blocks<L0, C0, 
     // thread 0 while the current tile's copy is in flight, read by all after the tile), then the
     // "last block" flag
     unsigned* shared_word = reinterpret_cast<unsigned*>(smem + BAR + 1);
-    float2* stage_tw = smem + BAR + 2;  // each tile's stage table (tma_shared_tw), then the end
     const int tid = threadIdx.x;
     if (smem_u32(smem) & 127) {  // bulk tensor copies need a 128-byte aligned destination
         if (tid == 0) *(volatile unsigned*)f.p0.err = 2u;
@@ -406,8 +396,8 @@ __global__ void __launch_bounds__(1 << (L0 + C0 - 4), (fused_min_blocks<L0, C0, 
             if (pass == 0) {
                 PassArgs a = f.p0;
                 a.inner_base = chunk << f.g;
-                ok = tma_tile<L0, C0, 0, false>(a, &tin, &tin, tile, 0, smem, bar, stage_tw, parity, fresh, tid,
-                                                AlwaysReady(), fetch_next, publish);
+                ok = tma_tile<L0, C0, 0, false>(a, &tin, &tin, tile, 0, smem, bar, parity, fresh, tid, AlwaysReady(),
+                                                fetch_next, publish);
                 if (ok) pending = (int)chunk;
             } else {
                 publish();
@@ -423,8 +413,8 @@ __global__ void __launch_bounds__(1 << (L0 + C0 - 4), (fused_min_blocks<L0, C0, 
                 };
                 PassArgs a = f.p1;
                 a.outer_base = chunk << f.g;
-                ok = tma_tile<L1, C1, 1, false>(a, &tmid, &tmid, tile, 0, smem, bar, stage_tw, parity, fresh, tid,
-                                                chunk_ready, fetch_next);
+                ok = tma_tile<L1, C1, 1, false>(a, &tmid, &tmid, tile, 0, smem, bar, parity, fresh, tid, chunk_ready,
+                                                fetch_next);
             }
             if (!ok) break;  // block-uniform: an expired wait, recorded in the error word
             parity ^= 1u;
@@ -595,10 +585,8 @@ bool pass01_fused_supported(int l0, int c0, int l1, int c1) {
 template <int L0, int C0, int L1, int C1>
 static cudaError_t launch_fused_t(const FusedArgs& f, int log2n, cudaStream_t stream) {
     constexpr int THREADS = 1 << (L0 + C0 - 4);
-    constexpr int BAR = tma_bar_offset(L0, C0) > tma_bar_offset(L1, C1) ? tma_bar_offset(L0, C0)
-                                                                        : tma_bar_offset(L1, C1);
-    constexpr int TW = tma_shared_tw(L0) > tma_shared_tw(L1) ? tma_shared_tw(L0) : tma_shared_tw(L1);
-    constexpr int SMEM = (int)sizeof(float2) * (BAR + 2 + TW) + 16;
+    constexpr int SMEM = tma_smem_bytes(L0, C0) > tma_smem_bytes(L1, C1) ? tma_smem_bytes(L0, C0)
+                                                                        : tma_smem_bytes(L1, C1);
     auto kernel = k_pass01_fused<L0, C0, L1, C1>;
     static std::atomic<unsigned long long> done{0};
     cudaError_t e = smem_limit((const void*)kernel, SMEM, done);
