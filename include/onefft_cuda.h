@@ -96,6 +96,10 @@ ONEFFT_API onefft_plan *onefft_plan_create_split(size_t n, int npass, const int 
  * such a kernel and the buffers are 16-byte aligned), and, for three passes, log2_chunk > 0 to
  * run the first two passes chunk by chunk over 2^log2_chunk columns of the last digit so that
  * each chunk's intermediate values stay in L2 (0 = whole passes). */
+/* npass = 1 at n = 2^12 or 2^13, log2_cols[0] = ONEFFT_COLS_PIPELINED: a persistent kernel with one
+ * transform per block that brings the next transform in by one bulk copy while computing the
+ * current one (for 16-byte aligned buffers; results equal the other widths bit for bit). */
+#define ONEFFT_COLS_PIPELINED 15
 #define ONEFFT_OPT_L2_KEEP 1
 #define ONEFFT_OPT_TMA 2
 /* ONEFFT_OPT_FUSED (three passes, log2_chunk > 0, with ONEFFT_OPT_TMA): the first two passes run

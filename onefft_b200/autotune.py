@@ -181,11 +181,17 @@ def time_plan(plan, x, y, reps: int, flush) -> float:
     return ts[len(ts) // 2]
 
 
+# ONEFFT_COLS_PIPELINED: the persistent double-buffered one-kernel form of 2^12 and 2^13
+PIPELINED = 15
+
+
 def batched_log_c_candidates(l: int) -> list[int]:
     """Transforms per block (log2) compiled for the one-kernel size 2^l (fft_kernels.cu,
-    batched_log_c_supported): the default 4096 / n, half and twice that up to 8192 values."""
+    batched_log_c_supported): the default 4096 / n, half and twice that up to 8192 values; at 2^12
+    and 2^13 also the pipelined form (fft_tma.cu, batched_pipe_supported)."""
     b = max(0, 12 - l)
-    return [c for c in (b - 1, b, b + 1) if c == b or (c >= 0 and l + c <= 13)]
+    out = [c for c in (b - 1, b, b + 1) if c == b or (c >= 0 and l + c <= 13)]
+    return out + ([PIPELINED] if l in (12, 13) else [])
 
 
 def tune_batched(reps: int = 9) -> dict:
@@ -227,8 +233,9 @@ def tune_batched(reps: int = 9) -> dict:
             times[c] = ts[len(ts) // 2]
         best = min(times, key=times.get)
         out[l] = {"log_c": best, "us": times}
-        print(f"batched 2^{l} x {batch}: " + ", ".join(f"{1 << c}/block {t:.1f} us" for c, t in times.items()) +
-              f" -> {1 << best}", flush=True)
+        label = lambda c: "pipelined" if c == PIPELINED else f"{1 << c}/block"  # noqa: E731
+        print(f"batched 2^{l} x {batch}: " + ", ".join(f"{label(c)} {t:.1f} us" for c, t in times.items()) +
+              f" -> {label(best)}", flush=True)
         del x, ref, y
         torch.cuda.empty_cache()
     table = [-1] * 15

@@ -84,6 +84,13 @@ cudaError_t set_expire_waits(int on);
 // passes 0 and 1 (ntiles = tiles per chunk; the per-chunk bases are ignored); one transform.
 // ctr: 2 + 2^(len2 - g) zeroed words used by no concurrent launch (zero again afterwards).
 bool pass01_fused_supported(int l0, int c0, int l1, int c1);
+// One-kernel sizes 2^12 / 2^13 as a persistent kernel with one transform per block and the next
+// transform's values arriving by one bulk copy while the current one computes (fft_tma.cu,
+// k_batched_pipe); same bits as launch_single_kernel. `in` 16-byte aligned; err: the plan's error
+// word (an expired copy wait).
+bool batched_pipe_supported(int log2n);
+cudaError_t launch_batched_pipe(int log2n, const float2* in, float2* out, long long batch, const float2* stw,
+                                int inverse, unsigned* err, cudaStream_t stream);
 cudaError_t launch_pass01_fused(int l0, int c0, int l1, int c1, const PassArgs& a0, const PassArgs& a1, int g,
                                 int len2, int lag, unsigned* ctr, cudaStream_t stream);
 cudaError_t launch_pass_tma(int mode, int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t stream);

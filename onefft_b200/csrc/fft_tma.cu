@@ -439,6 +439,80 @@ __global__ void __launch_bounds__(1 << (L0 + C0 - 4), (fused_min_blocks<L0, C0, 
     }
 }
 
+// ---- one-kernel sizes as a persistent, double-buffered pipeline ---------------------------------
+//
+// A whole transform of 2^LOG_L values per block, as k_batched, but the block stays resident and
+// walks the batch (transform blockIdx.x, then every gridDim.x-th): while it computes one
+// transform, the next one's 8 * 2^LOG_L bytes arrive in its second buffer through ONE bulk copy
+// (cp.async.bulk, completing on that buffer's mbarrier). A transform of 2^13 fills a block of 512
+// threads and half its SM's shared memory, so k_batched runs two of them per SM, each waiting for
+// its own loads; here the load of the next transform overlaps the arithmetic of this one. The
+// values then go from the dense buffer to registers and through the same Stockham stages
+// (tile_fft) as k_batched, so results equal it bit for bit. Buffers are padded for the exchanges
+// (which reuse them once the values are in registers); the two mbarriers follow them.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+template <int LOG_L>
+constexpr int pipe_smem_bytes() {
+    return 2 * (int)sizeof(float2) * ((1 << LOG_L) + (1 << (LOG_L - 4))) + 2 * (int)sizeof(uint64_t);
+}
+
+template <int LOG_L, int INV>
+__global__ void __launch_bounds__(1 << (LOG_L - 4), 1)
+    k_batched_pipe(const float2* __restrict__ in, float2* __restrict__ out, long long batch,
+                   const float2* __restrict__ stw, unsigned* err) {
+    constexpr int L = 1 << LOG_L, T = L / 16, BUF = L + L / 16;
+    constexpr unsigned BYTES = (unsigned)(L * sizeof(float2));
+    extern __shared__ __align__(1024) float2 smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * BUF);
+    const int tid = threadIdx.x;
+    const long long stride = gridDim.x;
+    long long b = blockIdx.x;
+    if (b >= batch) return;
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_expect_tx(&bar[0], BYTES);
+        bulk_load(smem, in + (b << LOG_L), BYTES, &bar[0]);
+    }
+    __syncthreads();  // the barriers are initialised before anyone waits on them
+    for (int k = 0; b < batch; ++k, b += stride) {
+        float2* buf = smem + (k & 1) * BUF;
+        const bool next = b + stride < batch;
+        if (tid == 0 && next) {
+            // the other buffer was last read and written as iteration k - 1's exchange space
+            // (generic accesses, ordered before this by the barrier that ended it)
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(&bar[(k + 1) & 1], BYTES);
+            bulk_load(smem + ((k + 1) & 1) * BUF, in + ((b + stride) << LOG_L), BYTES, &bar[(k + 1) & 1]);
+        }
+        const bool ok = !g_expire_waits && mbar_wait(&bar[k & 1], (unsigned)(k >> 1) & 1u);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                *(volatile unsigned*)err = 4u;
+                // let the copies in flight land before the block's memory is released
+                mbar_wait(&bar[k & 1], (unsigned)(k >> 1) & 1u);
+                if (next) mbar_wait(&bar[(k + 1) & 1], (unsigned)((k + 1) >> 1) & 1u);
+            }
+            return;
+        }
+        float2 v[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = INV ? swap_ri(buf[tid + T * i]) : buf[tid + T * i];
+        __syncthreads();  // every value is in registers before the exchanges reuse the buffer
+        tile_fft<LOG_L, 1>(v, tid, stw, buf, 0);
+        float2* dst = out + (b << LOG_L) + tid;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) dst[T * i] = INV ? swap_ri(v[i]) : v[i];
+        __syncthreads();  // the buffer is free before it is refilled (iteration k + 1 issues into it)
+    }
+}
+
 // ---- host side ----------------------------------------------------------------------------------
 
 static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -630,6 +704,50 @@ cudaError_t launch_pass01_fused(int l0, int c0, int l1, int c1, const PassArgs& 
     OFB_FUSED_SHAPES(OFB_FUSED_CASE)
 #undef OFB_FUSED_CASE
     return cudaErrorInvalidValue;
+}
+
+}  // namespace ofb
+
+namespace ofb {
+
+// ---- the pipelined one-kernel sizes: host side ---------------------------------------------------
+
+bool batched_pipe_supported(int log2n) { return log2n == 12 || log2n == 13; }
+
+template <int LOG_L>
+static cudaError_t launch_pipe_t(const float2* in, float2* out, long long batch, const float2* stw, int inverse,
+                                 unsigned* err, cudaStream_t stream) {
+    constexpr int THREADS = 1 << (LOG_L - 4), SMEM = pipe_smem_bytes<LOG_L>();
+    auto kernel = inverse ? k_batched_pipe<LOG_L, 1> : k_batched_pipe<LOG_L, 0>;
+    static std::atomic<unsigned long long> done_fwd{0}, done_inv{0};
+    cudaError_t e = smem_limit((const void*)kernel, SMEM, inverse ? done_inv : done_fwd);
+    if (e != cudaSuccess) return e;
+    // persistent grid: the blocks that fit on the device at once (per device and direction)
+    static std::atomic<int> grid_of[2][64];
+    int dev = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    int grid = grid_of[inverse ? 1 : 0][dev & 63].load(std::memory_order_relaxed);
+    if (grid == 0) {
+        int per_sm = 0, sms = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, THREADS, SMEM)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        grid = per_sm * sms > 0 ? per_sm * sms : 1;
+        grid_of[inverse ? 1 : 0][dev & 63].store(grid, std::memory_order_relaxed);
+    }
+    if ((long long)grid > batch) grid = (int)batch;
+    kernel<<<grid, THREADS, SMEM, stream>>>(in, out, batch, stw, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batched_pipe(int log2n, const float2* in, float2* out, long long batch, const float2* stw,
+                                int inverse, unsigned* err, cudaStream_t stream) {
+    if (batch <= 0) return cudaSuccess;
+    if ((uintptr_t)in & 15) return cudaErrorInvalidValue;  // bulk copies start on 16-byte boundaries
+    switch (log2n) {
+    case 12: return launch_pipe_t<12>(in, out, batch, stw, inverse, err, stream);
+    case 13: return launch_pipe_t<13>(in, out, batch, stw, inverse, err, stream);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace ofb

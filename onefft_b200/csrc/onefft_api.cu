@@ -180,9 +180,15 @@ static Shape tuned_shape(int m) {
     return kTuned[m - 15];
 }
 
+// One kernel, cols[0] = this: the persistent pipelined kernel (launch_batched_pipe) instead of
+// k_batched (ONEFFT_COLS_PIPELINED in onefft_cuda.h).
+constexpr int kPipelinedCols = 15;
+
 static bool valid_shape(int m, const Shape &s) {
     if (s.npass == 1)
-        return s.len[0] == m && m <= kMaxSingleLog2 && (s.cols[0] == -1 || batched_log_c_supported(m, s.cols[0]));
+        return s.len[0] == m && m <= kMaxSingleLog2 &&
+               (s.cols[0] == -1 || batched_log_c_supported(m, s.cols[0]) ||
+                (s.cols[0] == kPipelinedCols && batched_pipe_supported(m)));
     if (s.npass < 2 || s.npass > 3) return false;
     int sum = 0;
     for (int p = 0; p < s.npass; ++p) {
@@ -438,6 +444,12 @@ static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *
     if (p->npass == 1) {
         g_launches.fetch_add(1);
         if (p->tc) return launch_single_kernel_tc(p->log2n, in, out, batch, p->stw[0], inverse, p->tc, s);
+        if (p->cols[0] == kPipelinedCols) {
+            // bulk copies need 16-byte aligned transforms; weighted calls use k_batched's weights
+            if (!pre && !post && !((uintptr_t)in & 15))
+                return launch_batched_pipe(p->log2n, in, out, batch, p->stw[0], inverse, p->err, s);
+            return launch_single_kernel(p->log2n, in, out, batch, p->stw[0], inverse, s, pre, post, -1);
+        }
         return launch_single_kernel(p->log2n, in, out, batch, p->stw[0], inverse, s, pre, post, p->cols[0]);
     }
     PassArgs a{};

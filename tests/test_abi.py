@@ -138,7 +138,7 @@ def test_batched_width_rule_matches_autotuner(cuda_lib):
     from onefft_b200.autotune import batched_log_c_candidates
     for log2n in range(4, 15):
         ok = set(batched_log_c_candidates(log2n)) | {-1}
-        for c in range(-3, 12):
+        for c in range(-3, 17):
             lens = (ctypes.c_int * 1)(log2n)
             cols = (ctypes.c_int * 1)(c)
             h = cuda_lib.onefft_plan_create_tiles(1 << log2n, 1, lens, cols, 0, 0)
@@ -161,3 +161,18 @@ def test_autotuner_candidates_are_valid_splits(cuda_lib):
                 cuda_lib.onefft_plan_destroy(h)
             else:
                 assert b"invalid pass split" not in cuda_lib.onefft_last_error(), (m, lens, cols, chunk)
+
+
+def test_fused_candidates_are_valid_shapes(cuda_lib):
+    """Every fused shape the autotuner times (onefft_b200.autotune.fused_candidates: the first two
+    passes as one persistent kernel) passes the library's validation."""
+    from onefft_b200.autotune import fused_candidates
+    for m in (22, 24, 27, 30):
+        for lens, cols, chunk, lag in fused_candidates(m):
+            opts = 2 | 4 | (lag << 8)  # ONEFFT_OPT_TMA | ONEFFT_OPT_FUSED | ONEFFT_OPT_LAG(lag)
+            h = cuda_lib.onefft_plan_create_tiles(1 << m, 3, (ctypes.c_int * 3)(*lens), (ctypes.c_int * 3)(*cols),
+                                                  opts, chunk)
+            if h:
+                cuda_lib.onefft_plan_destroy(h)
+            else:
+                assert b"invalid pass split" not in cuda_lib.onefft_last_error(), (m, lens, cols, chunk, lag)

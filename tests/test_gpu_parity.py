@@ -385,3 +385,29 @@ def test_max_abs_report(ofb):
     """Prints the per-size max-abs errors gathered by test_size (the parity rule states them per size)."""
     for (l, d), v in sorted(MAX_ABS.items()):
         print(f"n=2^{l} {d}: max-abs {v:.3g}")
+
+
+@pytest.mark.parametrize("log2n", [12, 13])
+@pytest.mark.parametrize("batch", [5, 3001])
+def test_pipelined_one_kernel_equals_default(ofb, log2n, batch):
+    """The persistent double-buffered one-kernel form (ONEFFT_COLS_PIPELINED: the next
+    transform's values arrive by one bulk copy while the current one computes) gives the default
+    kernel's bits, for batches smaller than its grid and several times larger, both directions;
+    8-byte aligned buffers take the default kernel instead (same bits again)."""
+    import torch as T
+    n = 1 << log2n
+    pipe = ofb.Plan(n, split=(log2n,), cols=(15,))
+    ref = ofb.Plan(n)
+    g = T.Generator(device="cuda").manual_seed(log2n * 7 + batch)
+    buf = T.randn(2 * n * batch + 2, device="cuda", generator=g)
+    for off in (0, 2):  # 16-byte aligned, then 8-byte aligned
+        x = buf[off:off + 2 * n * batch]
+        a, b = T.empty_like(x), T.empty_like(x)
+        for inv in (False, True):
+            (pipe.dev_inverse if inv else pipe.dev_forward)(x.data_ptr(), a.data_ptr(), batch)
+            (ref.dev_inverse if inv else ref.dev_forward)(x.data_ptr(), b.data_ptr(), batch)
+            T.cuda.synchronize()
+            assert pipe.status() == 0
+            assert T.equal(a, b), (log2n, batch, off, inv)
+    pipe.destroy()
+    ref.destroy()
