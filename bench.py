@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-configs", action="store_true")
+    ap.add_argument("--e2e-schedule", default="pairs", choices=["pairs", "chains"],
+                    help="host threads of the end-to-end measurement (see the e2e section)")
     return ap.parse_args()
 
 
@@ -572,6 +574,30 @@ def main():
             for f in futs:
                 f.result()
 
+        def e2e_chains_run(k):
+            # Per item two chains, each running whole steps (forward, then inverse of its result)
+            # on its own buffers: chain c takes steps c, c + 2, ... The second chain starts about
+            # one upload later, so that while one chain copies a call's input to the device the
+            # other copies a result back, and the two keep that offset (their work is equal).
+            futs = []
+            for (w, hx, hy, hz), (pf, pi) in zip(host, pools):
+                up_s = 8.0 * (1 << w["log2n"]) * w["batch"] / 50e9  # one input at ~50 GB/s
+
+                def chain(c, w=w, hx=hx, hy=hy, hz=hz, up_s=up_s):
+                    if c:
+                        time.sleep(up_s)
+                    for s in range(c, k, 2):
+                        call(w, hx, hy[c], False)
+                        call(w, hy[c], hz[c], True)
+
+                futs += [pf.submit(chain, 0), pi.submit(chain, 1)]
+            for f in futs:
+                f.result()
+
+        if args.e2e_schedule == "chains":
+            for i, (w, hx, hy, hz) in enumerate(host):  # one result buffer per chain
+                host[i] = (w, hx, hy, [hz, torch.empty_like(hz, pin_memory=True)])
+            e2e_steps_run = e2e_chains_run  # noqa: F811
         e2e_steps_run(2)  # per-thread streams and staging buffers are set up here
         e2e_steps = max(2, min(args.steps, 12))
         torch.cuda.synchronize()
@@ -582,15 +608,20 @@ def main():
         t_e2e = (time.perf_counter() - t0) / e2e_steps
         t_e2e = max_over_ranks(t_e2e, device="cuda")
         same = all(torch.equal(hy[0][:4096].cuda(), w["y"][:4096]) and
-                   torch.equal(hz[:4096].cuda(), w["z"][:4096]) for w, hx, hy, hz in host)
+                   torch.equal((hz[0] if isinstance(hz, list) else hz)[:4096].cuda(), w["z"][:4096])
+                   for w, hx, hy, hz in host)
         nbytes = sum(2 * 8 * (1 << w["log2n"]) * w["batch"] for w in work)
         e2e = {"value": world * STEP_FLOPS / t_e2e / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes, "ms_per_step": 1e3 * t_e2e, "steps": e2e_steps,
                "matches_device_path": bool(same),
                "calls": "onefft_plan_forward/_inverse (single) and onefft_plan_forward/_inverse_batched (batch), "
                         "pinned host buffers",
-               "schedule": "per item one forward and one inverse host thread; step s+1's forward overlaps "
-                           "step s's inverse (intermediates double-buffered); time of all steps / steps"}
+               "schedule": ("per item one forward and one inverse host thread; step s+1's forward overlaps "
+                            "step s's inverse (intermediates double-buffered); time of all steps / steps")
+               if args.e2e_schedule == "pairs" else
+               ("per item two host threads, each running whole steps (forward, then inverse) on its own "
+                "buffers, the second started one upload later so one uploads while the other downloads; "
+                "time of all steps / steps")}
         for pf, pi in pools:
             pf.shutdown()
             pi.shutdown()
