@@ -75,6 +75,7 @@ def parse():
     ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--e2e-schedule", default="pairs", choices=["pairs", "chains"],
                     help="host threads of the end-to-end measurement (see the e2e section)")
+    ap.add_argument("--e2e-chains", type=int, default=2, help="chains per item of --e2e-schedule chains")
     return ap.parse_args()
 
 
@@ -526,6 +527,8 @@ def main():
             host.append((w, hx, hy, torch.empty_like(hx, pin_memory=True)))
         pools = [(concurrent.futures.ThreadPoolExecutor(max_workers=1),
                   concurrent.futures.ThreadPoolExecutor(max_workers=1)) for _ in host]
+        nchain = max(2, args.e2e_chains)
+        chain_pools = [[concurrent.futures.ThreadPoolExecutor(max_workers=1) for _ in range(nchain)] for _ in host]
 
         def call(w, src, dst, inverse):
             h = w["plan"].handle
@@ -575,28 +578,28 @@ def main():
                 f.result()
 
         def e2e_chains_run(k):
-            # Per item two chains, each running whole steps (forward, then inverse of its result)
-            # on its own buffers: chain c takes steps c, c + 2, ... The second chain starts about
-            # one upload later, so that while one chain copies a call's input to the device the
-            # other copies a result back, and the two keep that offset (their work is equal).
+            # Per item `nchain` chains, each running whole steps (forward, then inverse of its
+            # result) on its own buffers: chain c takes steps c, c + nchain, ... Chain c starts c
+            # uploads' time later, so that while one chain copies a call's input to the device
+            # another copies a result back, and they keep that offset (their work is equal).
             futs = []
-            for (w, hx, hy, hz), (pf, pi) in zip(host, pools):
+            for (w, hx, hy, hz), pc in zip(host, chain_pools):
                 up_s = 8.0 * (1 << w["log2n"]) * w["batch"] / 50e9  # one input at ~50 GB/s
 
                 def chain(c, w=w, hx=hx, hy=hy, hz=hz, up_s=up_s):
-                    if c:
-                        time.sleep(up_s)
-                    for s in range(c, k, 2):
+                    time.sleep(c * up_s * 2.0 / nchain)
+                    for s in range(c, k, nchain):
                         call(w, hx, hy[c], False)
                         call(w, hy[c], hz[c], True)
 
-                futs += [pf.submit(chain, 0), pi.submit(chain, 1)]
+                futs += [pc[c].submit(chain, c) for c in range(nchain)]
             for f in futs:
                 f.result()
 
         if args.e2e_schedule == "chains":
-            for i, (w, hx, hy, hz) in enumerate(host):  # one result buffer per chain
-                host[i] = (w, hx, hy, [hz, torch.empty_like(hz, pin_memory=True)])
+            for i, (w, hx, hy, hz) in enumerate(host):  # per chain its own intermediate and result
+                hy = hy + [torch.empty_like(hx, pin_memory=True) for _ in range(nchain - len(hy))]
+                host[i] = (w, hx, hy, [hz] + [torch.empty_like(hz, pin_memory=True) for _ in range(nchain - 1)])
             e2e_steps_run = e2e_chains_run  # noqa: F811
         e2e_steps_run(2)  # per-thread streams and staging buffers are set up here
         e2e_steps = max(2, min(args.steps, 12))
@@ -625,6 +628,9 @@ def main():
         for pf, pi in pools:
             pf.shutdown()
             pi.shutdown()
+        for pc in chain_pools:
+            for p in pc:
+                p.shutdown()
         del host
 
     # ---- the other configurations, measured beside the headline (rank 0, N = 1) ----
