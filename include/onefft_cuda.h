@@ -189,6 +189,38 @@ ONEFFT_API int onefft_uneven_status(onefft_uneven *batch);
 ONEFFT_API int onefft_uneven_execute_noalloc(const onefft_desc *desc, size_t count, const float *d_in, float *d_out,
                                              void *stream);
 
+/* ---- column transforms (the local steps of a transform distributed over several GPUs) -------
+ *
+ * The transforms down the `cols` columns of a row-major n x cols matrix,
+ *     Y_b[k] = sum_j in[j cols + b] w_n^(j k)          (0 <= b < cols, 0 <= k < n),
+ * optionally multiplied by the four-step twiddle of a larger transform of N = big_n values,
+ *     Y_b[k] *= w_N^((col0 + b) k),
+ * and written row-wise, split into `blocks` blocks of n / blocks consecutive outputs:
+ *     out[((k / r) cols + b) r + k mod r] = Y_b[k],    r = n / blocks.
+ * With blocks = 1 column b's results are row b of a cols x n matrix. OneFFT has no counterpart:
+ * these are the two local steps of the four-step transform of N = n1 n2 values over P ranks
+ * (onefft_b200/distributed.py): (1) each rank's n1 x (n2 / P) column block with n = n1,
+ * blocks = P, big_n = N, col0 = rank n2 / P writes the all-to-all send buffer directly; (2) the
+ * received n2 x (n1 / P) matrix with n = n2 gives the rank's n1 / P rows of the result. The
+ * twiddles follow OneFFT's rule (FP64, rounded once); swap flags give the inverse as
+ * swap(F(swap(x))) across the two steps.
+ *
+ * Sizes: n a power of two in [16, 2^24] (one kernel up to 2^12, two beyond, with an n x cols
+ * work buffer held by the object); cols a power of two >= 16 with n cols <= 2^31; blocks a power
+ * of two <= n; big_n 0 (no factor) or a power of two in [n, 2^40] with col0 + cols <= big_n / n.
+ * NULL / -1 for invalid sizes, as onefft_plan_create. */
+typedef struct onefft_columns onefft_columns;
+ONEFFT_API onefft_columns *onefft_columns_create(size_t n, size_t cols, size_t blocks, unsigned long long big_n,
+                                                 unsigned long long col0);
+ONEFFT_API void onefft_columns_destroy(onefft_columns *columns);
+/* flags: ONEFFT_SWAP_IN exchanges re/im of the input as it is read, ONEFFT_SWAP_OUT of the
+ * result as it is written (after the twiddle). d_in / d_out: n cols complex values each, 8-byte
+ * aligned device pointers, not overlapping. Enqueue only, like the other device entry points. */
+#define ONEFFT_SWAP_IN 1
+#define ONEFFT_SWAP_OUT 2
+ONEFFT_API int onefft_columns_execute(const onefft_columns *columns, const float *d_in, float *d_out, int flags,
+                                      void *stream);
+
 /* ---- information and testing hooks -------------------------------------------------------------*/
 
 /* Message of the last error in the calling thread ("" if none). */

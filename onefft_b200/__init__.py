@@ -38,6 +38,7 @@ C_SYMBOLS = (
     "onefft_uneven_create", "onefft_uneven_create_split", "onefft_uneven_destroy", "onefft_uneven_span", "onefft_uneven_execute",
     "onefft_uneven_status",
     "onefft_uneven_execute_noalloc",
+    "onefft_columns_create", "onefft_columns_destroy", "onefft_columns_execute",
     "onefft_last_error", "onefft_plan_status", "onefft_debug_fail_alloc", "onefft_debug_twiddles",
     "onefft_debug_launch_count", "onefft_debug_expire_waits",
 )
@@ -113,6 +114,12 @@ def lib() -> ctypes.CDLL:
     L.onefft_uneven_status.restype = ctypes.c_int
     L.onefft_uneven_execute_noalloc.argtypes = [_vp, _sz, _vp, _vp, _vp]
     L.onefft_uneven_execute_noalloc.restype = ctypes.c_int
+    L.onefft_columns_create.argtypes = [_sz, _sz, _sz, ctypes.c_ulonglong, ctypes.c_ulonglong]
+    L.onefft_columns_create.restype = _vp
+    L.onefft_columns_destroy.argtypes = [_vp]
+    L.onefft_columns_destroy.restype = None
+    L.onefft_columns_execute.argtypes = [_vp, _vp, _vp, ctypes.c_int, _vp]
+    L.onefft_columns_execute.restype = ctypes.c_int
     L.onefft_last_error.argtypes = []
     L.onefft_last_error.restype = ctypes.c_char_p
     L.onefft_debug_fail_alloc.argtypes = [ctypes.c_int]
@@ -362,5 +369,43 @@ class UnevenBatch:
             pass
 
 
-__all__ = ["forward", "inverse", "cache_prepare", "cache_clear", "Plan", "UnevenBatch", "DESC_DTYPE",
-           "implementation", "last_error", "lib", "LIB_PATH", "C_SYMBOLS"]
+SWAP_IN, SWAP_OUT = 1, 2  # ONEFFT_SWAP_IN / ONEFFT_SWAP_OUT
+
+
+class Columns:
+    """Transforms down the columns of a row-major n x cols matrix, written row-wise in `blocks`
+    blocks, optionally times the four-step twiddle w_big_n^((col0 + b) k) of a larger transform
+    (onefft_columns_* in include/onefft_cuda.h): out[((k / r) cols + b) r + k mod r] = Y_b[k],
+    r = n / blocks."""
+
+    def __init__(self, n: int, cols: int, blocks: int = 1, big_n: int = 0, col0: int = 0):
+        h = lib().onefft_columns_create(n, cols, blocks, big_n, col0)
+        if not h:
+            raise ValueError(f"no column transform for n={n}, cols={cols}, blocks={blocks}, big_n={big_n}, "
+                             f"col0={col0}: {last_error()}")
+        self._h = h
+        self.n, self.cols, self.blocks, self.big_n, self.col0 = int(n), int(cols), int(blocks), int(big_n), int(col0)
+
+    def execute(self, d_in: int, d_out: int, flags: int = 0, stream: int = 0) -> None:
+        """Enqueues the transform of n * cols complex values at d_in into d_out (device pointers;
+        flags: SWAP_IN | SWAP_OUT)."""
+        if not self._h:
+            raise ValueError("column transform was destroyed")
+        rc = lib().onefft_columns_execute(self._h, d_in, d_out, flags, stream)
+        if rc != 0:
+            raise RuntimeError(f"onefft_columns_execute failed ({rc}): {last_error()}")
+
+    def destroy(self) -> None:
+        if getattr(self, "_h", None):
+            lib().onefft_columns_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+__all__ = ["forward", "inverse", "cache_prepare", "cache_clear", "Plan", "UnevenBatch", "DESC_DTYPE", "Columns",
+           "SWAP_IN", "SWAP_OUT", "implementation", "last_error", "lib", "LIB_PATH", "C_SYMBOLS"]

@@ -138,10 +138,11 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4))
     }
 }
 
-template <int LOG_L, int LOG_C, int MODE, bool W>
+template <int LOG_L, int LOG_C, int MODE, bool W, bool X = false>
 __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4)) k_pass(PassArgs a) {
     extern __shared__ float2 smem[];
-    pass_tile<LOG_L, LOG_C, MODE, false, W>(a, blockIdx.x, (long long)blockIdx.y << a.log2n, smem, threadIdx.x);
+    pass_tile<LOG_L, LOG_C, MODE, 0, W, false, X>(a, blockIdx.x, X ? 0ll : (long long)blockIdx.y << a.log2n, smem,
+                                                  threadIdx.x);
 }
 
 // ---- launchers -------------------------------------------------------------------------------------
@@ -239,7 +240,9 @@ cudaError_t launch_single_kernel(int log2n, const float2* in, float2* out, long 
 // Default tile width (columns per block) of a pass of length 2^log_l: 16 columns (one 128-byte
 // line per row) up to 512 points, then 8 at 1024 and 4 beyond, so a tile holds at most 16384
 // values (136 KiB of shared memory with padding at 4 x 4096).
-int pass_log_c(int log_l) { return log_l <= 9 ? 4 : log_l == 10 ? 3 : 2; }
+constexpr int default_pass_log_c(int log_l) { return log_l <= 9 ? 4 : log_l == 10 ? 3 : 2; }
+
+int pass_log_c(int log_l) { return default_pass_log_c(log_l); }
 
 // Tile widths compiled for each pass length: 2^2 .. 2^4 columns with at most 16384 values, and
 // 2 columns for lengths 2^10 .. 2^12 (two tiles of adjacent blocks then share each 32-byte
@@ -319,6 +322,43 @@ cudaError_t launch_pass(int mode, int log_l, int log_c, const PassArgs& a, int b
     case 1: return launch_pass_mode<1>(log_l, log_c, a, batch, stream);
     default: return launch_pass_mode<2>(log_l, log_c, a, batch, stream);
     }
+}
+
+// Column transforms: one launch over the whole matrix, default tile width, twiddle rows in
+// shared memory in both modes.
+template <int LOG_L, int MODE>
+static cudaError_t launch_columns_t(const PassArgs& a, cudaStream_t stream) {
+    constexpr int LOG_C = default_pass_log_c(LOG_L);
+    constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
+    constexpr int SMEM = pass_smem_bytes(LOG_L, LOG_C, 1);
+    auto kernel = k_pass<LOG_L, LOG_C, MODE, false, true>;
+    static std::atomic<unsigned long long> done{0};
+    const cudaError_t attr = smem_limit((const void*)kernel, SMEM, done);
+    if (attr != cudaSuccess) return attr;
+    if (a.log2n > 31 || a.log2n < LOG_L + LOG_C) return cudaErrorInvalidValue;
+    PassArgs b = a;
+    b.tli = 31;
+    kernel<<<1u << (a.log2n - LOG_L - LOG_C), THREADS, SMEM, stream>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pass_columns(int mode, int log_l, const PassArgs& a, cudaStream_t stream) {
+    if (mode != 0 && mode != 2) return cudaErrorInvalidValue;
+#define OFB_COLUMNS_CASE(LL) \
+    case LL: return mode == 0 ? launch_columns_t<LL, 0>(a, stream) : launch_columns_t<LL, 2>(a, stream);
+    switch (log_l) {
+        OFB_COLUMNS_CASE(4)
+        OFB_COLUMNS_CASE(5)
+        OFB_COLUMNS_CASE(6)
+        OFB_COLUMNS_CASE(7)
+        OFB_COLUMNS_CASE(8)
+        OFB_COLUMNS_CASE(9)
+        OFB_COLUMNS_CASE(10)
+        OFB_COLUMNS_CASE(11)
+        OFB_COLUMNS_CASE(12)
+    default: return cudaErrorInvalidValue;
+    }
+#undef OFB_COLUMNS_CASE
 }
 
 int stage_table_entries_host(int log_l) { return stage_table_entries(log_l); }

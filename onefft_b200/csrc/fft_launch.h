@@ -52,6 +52,19 @@ struct PassArgs {
     // i by pre[i], the last pass output element i (natural order) by post[i]
     const float2* pre;
     const float2* post;
+    // Column transforms (launch_pass_columns only; zero elsewhere). The launch covers one matrix
+    // of 2^log2n values whose columns are 2^xlog_cols interleaved transforms:
+    //  - tw_shift: the first pass's inter-pass factor of column col is F = xcol0 + (col >> tw_shift),
+    //    its tables (tw_lo, tw_hi, lo_bits) those of w_(2^xlog2n); tw_lo NULL = no factor;
+    //  - the last pass multiplies output k of transform h by w_(2^xlog2n)^((xcol0 + h) k);
+    //  - colstore: output k of transform b goes to
+    //    ((((k >> xlog_blk) << xlog_cols) + b) << xlog_blk) + (k mod 2^xlog_blk).
+    int tw_shift;
+    int xlog2n;
+    unsigned long long xcol0;
+    int colstore;
+    int xlog_blk;
+    int xlog_cols;
 };
 
 // Largest size handled by one kernel (k_tiny / k_batched).
@@ -72,6 +85,10 @@ cudaError_t launch_single_kernel(int log2n, const float2* in, float2* out, long 
                                  int inverse, cudaStream_t stream, const float2* pre = nullptr,
                                  const float2* post = nullptr, int log_c = -1);
 cudaError_t launch_pass(int mode, int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t stream);
+// One pass (mode 0 first, 2 last) of a column transform (see the column fields of PassArgs), with
+// the default tile width pass_log_c(log_l); one launch over the whole matrix of 2^a.log2n values
+// (log2n <= 31, at least one tile).
+cudaError_t launch_pass_columns(int mode, int log_l, const PassArgs& a, cudaStream_t stream);
 // TMA-staged passes (fft_tma.cu): same arithmetic as launch_pass; 16-byte aligned buffers,
 // batch <= 65535, shapes pass_tma_supported()
 bool pass_tma_supported(int log_l, int log_c);

@@ -56,6 +56,47 @@ __device__ __forceinline__ float2 pass_twiddle_lane(const PassArgs& a, unsigned 
     return make_float2((float)w.x, (float)w.y);
 }
 
+// Column transforms (PassArgs' column fields): w_N^t, N = 2^a.xlog2n <= 2^40, for any 64-bit t
+// (reduced mod N; unsigned products wrap mod 2^64, a multiple of N).
+__device__ __forceinline__ double2 wide_twiddle_f64(const PassArgs& a, unsigned long long t) {
+    t &= (1ull << a.xlog2n) - 1;
+    return zmul(__ldg(a.tw_lo + (t & ((1ull << a.lo_bits) - 1))), __ldg(a.tw_hi + (t >> a.lo_bits)));
+}
+// The factors of a column-transform tile, split like the inter-pass twiddles above (one FP32
+// rounding per factor). First pass: output j + T kk of column col gets w_N^(F (j + T kk)),
+// F = xcol0 + (col >> tw_shift): rows w_N^(F T kk) per column, lane w_N^(F j). Last pass: output
+// k = q + 2^log_s (j + T kk) of transform h = col >> log_s (q = col mod 2^log_s) gets
+// w_N^((xcol0 + h) k): rows w_N^((xcol0 + h) 2^log_s T kk), one per tile (a tile's columns share
+// h), lane w_N^((xcol0 + h)(q + 2^log_s j)).
+template <int LOG_L, int LOG_C, int MODE>
+__device__ __forceinline__ void column_twiddle_rows(const PassArgs& a, unsigned col0, float2* tws, int tid, int nthreads) {
+    constexpr unsigned long long T = 1ull << (LOG_L - 4);
+    constexpr int C = 1 << LOG_C;
+    for (int i = tid; i < (MODE == 0 ? C : 1) * 16; i += nthreads) {
+        const int cc = i >> 4, kk = i & 15;
+        const unsigned long long step = MODE == 0 ? (a.xcol0 + ((col0 + cc) >> a.tw_shift)) * T
+                                                  : ((a.xcol0 + (col0 >> a.log_s)) << a.log_s) * T;
+        const double2 w = zpow<4>(wide_twiddle_f64(a, step), (unsigned)kk);
+        tws[cc * 17 + kk] = make_float2((float)w.x, (float)w.y);
+    }
+}
+template <int LOG_L, int MODE>
+__device__ __forceinline__ float2 column_twiddle_lane(const PassArgs& a, unsigned col0, int c, int j) {
+    double2 w;
+    if (MODE == 0) {
+        w = zpow<LOG_L - 4>(wide_twiddle_f64(a, a.xcol0 + ((col0 + c) >> a.tw_shift)), (unsigned)j);
+    } else {
+        const unsigned long long f = a.xcol0 + (col0 >> a.log_s);
+        const unsigned long long q = (col0 & ((1u << a.log_s) - 1)) + c;
+        w = wide_twiddle_f64(a, f * (q + ((unsigned long long)j << a.log_s)));
+    }
+    return make_float2((float)w.x, (float)w.y);
+}
+// Destination of output k of transform b in the column layout (PassArgs::colstore).
+__device__ __forceinline__ long long column_dst(const PassArgs& a, unsigned long long b, unsigned long long k) {
+    return (long long)(((((k >> a.xlog_blk) << a.xlog_cols) + b) << a.xlog_blk) + (k & ((1ull << a.xlog_blk) - 1)));
+}
+
 // Loads of data the kernel never writes go through the read-only path; the intermediate array
 // between passes may be kept in L2 for the next pass (evict last).
 __device__ __forceinline__ float2 ld_stream(const float2* p) { return __ldg(p); }
@@ -184,7 +225,11 @@ __device__ __forceinline__ void batched_tile(const float2* __restrict__ src, flo
 // CG: later passes load through L2 only (ld.global.cg), for data that other blocks of the same
 // launch wrote: an SM's L1 may still hold an older copy of a line that it read for a neighbouring
 // transform.
-template <int LOG_L, int LOG_C, int MODE, int TC = 0, bool W = false, bool CG = false>
+// X: a pass of a column transform (PassArgs' column fields): MODE 0 takes its inter-pass factor
+// from the column fields and, with colstore, writes the column layout (and a.swap_out: it is
+// then the only pass); MODE 2 reads a.in, multiplies by the larger transform's factors and
+// writes the column layout to a.out. One matrix per launch (toff 0).
+template <int LOG_L, int LOG_C, int MODE, int TC = 0, bool W = false, bool CG = false, bool X = false>
 __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long long toff, float2* smem, int tid) {
     constexpr int L = 1 << LOG_L, T = L / 16, C = 1 << LOG_C;
     const int c = tid & (C - 1);
@@ -207,7 +252,14 @@ __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long lo
     // FP32 (pass_twiddle_rows / pass_twiddle_lane).
     float2* tws = smem + spad(C * L - 1) + 1;
     float2 wjf = make_float2(1.f, 0.f);
-    if (MODE != 2) {
+    bool twiddled = MODE != 2;
+    if constexpr (X) {
+        twiddled = MODE != 1 && a.tw_lo != nullptr;  // the same for the whole block
+        if (twiddled) {
+            column_twiddle_rows<LOG_L, LOG_C, MODE>(a, col0, tws, tid, C * T);
+            wjf = column_twiddle_lane<LOG_L, MODE>(a, col0, c, j);
+        }
+    } else if (MODE != 2) {
         pass_twiddle_rows<LOG_L, LOG_C, MODE>(a, col0, tws, tid, C * T);
         wjf = pass_twiddle_lane<LOG_L>(a, MODE == 0 ? col0 + c : (col0 >> a.log_s) << a.log_s, j);
     }
@@ -230,7 +282,7 @@ __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long lo
     }
     if constexpr (TC != 0) tile_fft_tc<LOG_L, LOG_C, C, TC>(v, j, a.stw, smem, c, tid);
     else tile_fft<LOG_L, C>(v, j, a.stw, smem, c);
-    if (MODE != 2) {
+    if (twiddled) {
         if (Stages<LOG_L>::COUNT == 1) __syncthreads();  // tile_fft had no barrier to publish tws
         const float2* tw = tws + (MODE == 0 ? c * 17 : 0);
 #pragma unroll
@@ -249,6 +301,15 @@ __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long lo
         __syncthreads();
         const int cc = tid >> (LOG_L - 4), kk0 = tid & (T - 1);
         const unsigned rr = col0 + cc;
+        if (X && a.colstore) {
+            const float2* r = smem + spad(kk0 * C + cc);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const float2 x = r[padc(i * T * C)];
+                a.out[column_dst(a, rr, (unsigned)(kk0 + i * T))] = a.swap_out ? swap_ri(x) : x;
+            }
+            return;
+        }
         const unsigned j2 = rr & ((1u << a.rev_b2) - 1), j1 = rr >> a.rev_b2;
         float2* q = a.out + toff + (((j1 + (j2 << a.rev_b1)) << LOG_L) + kk0);
         const float2* r = smem + spad(kk0 * C + cc);
@@ -257,6 +318,13 @@ __device__ __forceinline__ void pass_tile(const PassArgs& a, unsigned t, long lo
             float2 x = r[padc(i * T * C)];
             if (a.l2_keep) st_policy(q + i * T, x, keep);
             else q[i * T] = x;
+        }
+    } else if (X && MODE == 2) {
+        const unsigned long long h = col0 >> a.log_s, q = (col0 & ((1u << a.log_s) - 1)) + c;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const float2 x = a.swap_out ? swap_ri(v[k]) : v[k];
+            a.out[column_dst(a, h, q + ((unsigned long long)(j + T * k) << a.log_s))] = x;
         }
     } else {
         float2* p0 = a.out + off0;

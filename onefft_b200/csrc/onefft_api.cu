@@ -1226,3 +1226,224 @@ extern "C" int onefft_uneven_execute(onefft_uneven *u, const float *d_in, float 
     }
     return e == cudaSuccess ? 0 : cuda_error(e, "uneven batch launch");
 }
+
+// ---- column transforms ------------------------------------------------------------------------
+//
+// One or two passes of the pass kernels over the whole n x cols matrix, seen as one array of
+// n cols values whose element (j, b) sits at j cols + b:
+//   one pass (n <= 2^12): transforms down the columns (stride cols), the larger transform's
+//     factor and the column-layout store in the same kernel;
+//   two passes n = 2^a 2^b: pass 0 transforms the top a bits of j (stride 2^b cols) with the
+//     n-point four-step factor w_n^(j1 k0) (j1 = the low digit, column index >> log2 cols) and
+//     writes column b's values as rows [b][j1][k0] of the work buffer, exactly the layout of a
+//     two-pass plan's first pass for a batch of cols transforms; pass 1 transforms j1 in each
+//     row block, multiplies by the larger transform's factor and writes the column layout.
+
+struct onefft_columns {
+    int device = 0;
+    int m = 0, lb = 0, log_blk = 0, log2big = 0;
+    int npass = 0, len[2] = {0, 0};
+    unsigned long long col0 = 0;
+    void *mem = nullptr;
+    const float2 *stw[2] = {nullptr, nullptr};
+    const double2 *tw_lo = nullptr, *tw_hi = nullptr;  // w_n (two passes)
+    int lo_bits = 0;
+    const double2 *big_lo = nullptr, *big_hi = nullptr;  // w_N (big_n > 0)
+    int big_lo_bits = 0;
+    float2 *work = nullptr;
+};
+
+static bool pow2_log(unsigned long long x, int *l) {
+    if (x == 0 || (x & (x - 1))) return false;
+    int k = 0;
+    while ((1ull << k) < x) ++k;
+    *l = k;
+    return true;
+}
+
+extern "C" onefft_columns *onefft_columns_create(size_t n, size_t cols, size_t blocks, unsigned long long big_n,
+                                                 unsigned long long col0) {
+    t_last_error.clear();
+    int m, lb, lk, lbig = 0;
+    if (!pow2_log(n, &m) || m < 4 || m > 24) {
+        set_error(ONEFFT_ERR_SIZE, "columns: n=%zu is not a power of two in [16, 2^24]", n);
+        return nullptr;
+    }
+    if (!pow2_log(cols, &lb) || lb < 4 || m + lb > 31) {
+        set_error(ONEFFT_ERR_SIZE, "columns: cols=%zu is not a power of two >= 16 with n cols <= 2^31", cols);
+        return nullptr;
+    }
+    if (!pow2_log(blocks, &lk) || lk > m) {
+        set_error(ONEFFT_ERR_SIZE, "columns: blocks=%zu is not a power of two <= n", blocks);
+        return nullptr;
+    }
+    if (big_n && (!pow2_log(big_n, &lbig) || lbig < m || lbig > 40 || col0 > (big_n >> m) ||
+                  cols > (big_n >> m) - col0)) {
+        set_error(ONEFFT_ERR_SIZE, "columns: big_n=%llu must be a power of two in [n, 2^40] with col0 + cols <= big_n / n",
+                  big_n);
+        return nullptr;
+    }
+    if (!big_n && col0) {
+        set_error(ONEFFT_ERR_SIZE, "columns: col0 without big_n");
+        return nullptr;
+    }
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) {
+        cuda_error(e, "no CUDA device");
+        return nullptr;
+    }
+    onefft_columns *c = new (std::nothrow) onefft_columns();
+    if (!c) {
+        set_error(ONEFFT_ERR_SIZE, "out of host memory");
+        return nullptr;
+    }
+    c->device = device;
+    c->m = m;
+    c->lb = lb;
+    c->log_blk = m - lk;
+    c->log2big = lbig;
+    c->col0 = col0;
+    c->npass = m <= 12 ? 1 : 2;
+    c->len[0] = c->npass == 1 ? m : (m + 1) / 2;
+    c->len[1] = c->npass == 1 ? 0 : m / 2;
+    // layout: stage tables, the w_n tables (two passes), the w_N tables, the work buffer
+    size_t off[2] = {0, 0}, bytes = 0;
+    for (int i = 0; i < c->npass; ++i) {
+        off[i] = bytes;
+        bytes = align256(bytes + sizeof(float2) * (size_t)stage_table_entries_host(c->len[i]));
+    }
+    size_t lo_off = 0, hi_off = 0, blo_off = 0, bhi_off = 0, work_off = 0;
+    if (c->npass == 2) {
+        c->lo_bits = m / 2;
+        lo_off = bytes;
+        bytes = align256(bytes + sizeof(double2) * ((size_t)1 << c->lo_bits));
+        hi_off = bytes;
+        bytes = align256(bytes + sizeof(double2) * ((size_t)1 << (m - c->lo_bits)));
+    }
+    if (lbig) {
+        c->big_lo_bits = lbig / 2;
+        blo_off = bytes;
+        bytes = align256(bytes + sizeof(double2) * ((size_t)1 << c->big_lo_bits));
+        bhi_off = bytes;
+        bytes = align256(bytes + sizeof(double2) * ((size_t)1 << (lbig - c->big_lo_bits)));
+    }
+    if (c->npass == 2) {
+        work_off = bytes;
+        bytes += sizeof(float2) << (m + lb);
+    }
+    e = dev_alloc(&c->mem, bytes);
+    if (e != cudaSuccess) {
+        delete c;
+        cuda_error(e, "column transform allocation");
+        set_error(ONEFFT_ERR_SIZE, "column transform allocation failed");
+        return nullptr;
+    }
+    char *base = (char *)c->mem;
+    cudaStream_t s = nullptr;
+    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        for (int i = 0; i < c->npass && e == cudaSuccess; ++i) {
+            c->stw[i] = (const float2 *)(base + off[i]);
+            e = launch_stage_table((float2 *)(base + off[i]), c->len[i], s);
+        }
+        if (c->npass == 2 && e == cudaSuccess) {
+            c->tw_lo = (const double2 *)(base + lo_off);
+            c->tw_hi = (const double2 *)(base + hi_off);
+            e = launch_big_table((double2 *)c->tw_lo, (double2 *)c->tw_hi, m, c->lo_bits, s);
+        }
+        if (lbig && e == cudaSuccess) {
+            c->big_lo = (const double2 *)(base + blo_off);
+            c->big_hi = (const double2 *)(base + bhi_off);
+            e = launch_big_table((double2 *)c->big_lo, (double2 *)c->big_hi, lbig, c->big_lo_bits, s);
+        }
+        if (c->npass == 2) c->work = (float2 *)(base + work_off);
+        cudaError_t e2 = cudaStreamSynchronize(s);
+        if (e == cudaSuccess) e = e2;
+        cudaStreamDestroy(s);
+    }
+    if (e != cudaSuccess) {
+        cudaFree(c->mem);
+        delete c;
+        cuda_error(e, "column transform table build");
+        return nullptr;
+    }
+    return c;
+}
+
+extern "C" void onefft_columns_destroy(onefft_columns *c) {
+    if (!c) return;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != c->device) cudaSetDevice(c->device);
+    cudaFree(c->mem);
+    if (cur >= 0 && cur != c->device) cudaSetDevice(cur);
+    delete c;
+}
+
+extern "C" int onefft_columns_execute(const onefft_columns *c, const float *d_in, float *d_out, int flags,
+                                      void *stream) {
+    t_last_error.clear();
+    if (!c) return set_error(ONEFFT_ERR_ARG, "NULL column transform");
+    if (!d_in || !d_out) return set_error(ONEFFT_ERR_ARG, "NULL buffer");
+    if (((uintptr_t)d_in | (uintptr_t)d_out) & 7) return set_error(ONEFFT_ERR_ARG, "device buffers must be 8-byte aligned");
+    if (flags & ~(ONEFFT_SWAP_IN | ONEFFT_SWAP_OUT)) return set_error(ONEFFT_ERR_ARG, "unknown flags %d", flags);
+    const size_t bytes = sizeof(float2) << (c->m + c->lb);
+    if (ranges_overlap(d_in, d_out, bytes)) return set_error(ONEFFT_ERR_ARG, "input and output overlap");
+    const cudaStream_t s = (cudaStream_t)stream;
+    PassArgs a{};
+    a.log2n = c->m + c->lb;
+    a.tli = 31;
+    a.swap_in = (flags & ONEFFT_SWAP_IN) ? 1 : 0;
+    a.xlog_blk = c->log_blk;
+    a.xlog_cols = c->lb;
+    cudaError_t e;
+    if (c->npass == 1) {
+        a.in = (const float2 *)d_in;
+        a.out = (float2 *)d_out;
+        a.log_s = c->lb;
+        a.stw = c->stw[0];
+        a.swap_out = (flags & ONEFFT_SWAP_OUT) ? 1 : 0;
+        a.tw_lo = c->big_lo;  // NULL: no factor
+        a.tw_hi = c->big_hi;
+        a.lo_bits = c->big_lo_bits;
+        a.xlog2n = c->log2big;
+        a.xcol0 = c->col0;
+        a.colstore = 1;
+        g_launches.fetch_add(1);
+        e = launch_pass_columns(0, c->len[0], a, s);
+    } else {
+        PassArgs p0 = a;
+        p0.in = (const float2 *)d_in;
+        p0.out = c->work;
+        p0.log_s = c->len[1] + c->lb;
+        p0.rev_b1 = c->len[1];
+        p0.rev_b2 = c->lb;
+        p0.stw = c->stw[0];
+        p0.tw_lo = c->tw_lo;
+        p0.tw_hi = c->tw_hi;
+        p0.lo_bits = c->lo_bits;
+        p0.xlog2n = c->m;
+        p0.tw_shift = c->lb;
+        g_launches.fetch_add(1);
+        e = launch_pass_columns(0, c->len[0], p0, s);
+        if (e == cudaSuccess) {
+            PassArgs p1 = a;
+            p1.in = c->work;
+            p1.out = (float2 *)d_out;
+            p1.swap_in = 0;
+            p1.swap_out = (flags & ONEFFT_SWAP_OUT) ? 1 : 0;
+            p1.log_s = c->len[0];
+            p1.stw = c->stw[1];
+            p1.tw_lo = c->big_lo;
+            p1.tw_hi = c->big_hi;
+            p1.lo_bits = c->big_lo_bits;
+            p1.xlog2n = c->log2big;
+            p1.xcol0 = c->col0;
+            p1.colstore = 1;
+            g_launches.fetch_add(1);
+            e = launch_pass_columns(2, c->len[1], p1, s);
+        }
+    }
+    return e == cudaSuccess ? 0 : cuda_error(e, "column transform launch");
+}

@@ -201,6 +201,26 @@ def fft64_numpy(x: np.ndarray, inverse: bool = False) -> np.ndarray:
     return np.ascontiguousarray(y).view(np.float64)
 
 
+def columns_fp64(x: np.ndarray, n: int, cols: int, blocks: int = 1, big_n: int = 0, col0: int = 0,
+                 flags: int = 0) -> np.ndarray:
+    """FP64 statement of the column transform's contract (onefft_columns_execute,
+    include/onefft_cuda.h): transforms down the columns of the n x cols matrix x (complex),
+    times w_big_n^((col0 + b) k), out[((k / r) cols + b) r + k mod r] = Y_b[k], r = n / blocks;
+    flags 1 / 2 exchange re/im of the input / of the result. Returns complex128. The exponent is
+    reduced modulo big_n in integers before the angle is formed."""
+    a = np.asarray(x).astype(np.complex128).reshape(n, cols)
+    if flags & 1:
+        a = a.imag + 1j * a.real
+    y = np.fft.fft(a, axis=0)
+    if big_n:
+        t = ((col0 + np.arange(cols, dtype=np.int64))[None, :] * np.arange(n, dtype=np.int64)[:, None]) % big_n
+        y = y * np.exp(-2j * np.pi * (t.astype(np.float64) / big_n))
+    if flags & 2:
+        y = y.imag + 1j * y.real
+    r = n // blocks
+    return np.ascontiguousarray(y.T.reshape(cols, blocks, r).transpose(1, 0, 2)).reshape(-1)
+
+
 def dft_bins(x: np.ndarray, bins, inverse: bool = False) -> np.ndarray:
     x = np.ascontiguousarray(x, np.float32)
     b = np.ascontiguousarray(np.asarray(bins, np.uint64))

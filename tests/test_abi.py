@@ -122,6 +122,17 @@ def test_uneven_descriptors_validated_on_host(cuda_lib):
     assert cuda_lib.onefft_uneven_execute(None, 0, 0, None) == -2
 
 
+def test_column_transform_shapes_validated_on_host(cuda_lib):
+    """onefft_columns_create rejects shapes outside its contract before any device work."""
+    import onefft_b200 as ofb
+    for args in [(8, 16), (1 << 25, 16), (256, 8), (256, 24), (256, 16, 512), (256, 16, 3), (256, 16, 1, 128),
+                 (256, 16, 1, 1 << 41), (256, 16, 1, 1 << 12, 1), (256, 16, 1, 0, 3), (1 << 20, 1 << 12)]:
+        with pytest.raises(ValueError):
+            ofb.Columns(*args)
+    assert cuda_lib.onefft_columns_execute(None, 0, 0, 0, None) == -2
+    cuda_lib.onefft_columns_destroy(None)
+
+
 def test_python_mirror_raises_on_invalid_size(cuda_lib):
     import onefft_b200
     with pytest.raises(ValueError):

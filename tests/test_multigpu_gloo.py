@@ -75,13 +75,16 @@ def test_two_ranks_shard_and_reduce(oracle):
     assert results[0][2] == results[1][2]
 
 
-def _numpy_fft_last_dim(t):
-    """CPU stand-in for the GPU kernels: FP64 FFT along the last dimension, back to complex64."""
+def cpu_columns(x, n, cols, blocks, big_n, col0, flags):
+    """CPU stand-in for the column-transform kernels: the oracle's FP64 statement of the same
+    contract, back to complex64."""
     import torch
-    return torch.from_numpy(np.fft.fft(t.numpy().astype(np.complex128), axis=-1).astype(np.complex64))
+
+    import oracle
+    return torch.from_numpy(oracle.columns_fp64(x.numpy(), n, cols, blocks, big_n, col0, flags).astype(np.complex64))
 
 
-def dist_worker(rank: int, world: int, port: int, n1: int, n2: int, q):
+def dist_worker(rank: int, world: int, port: int, n1: int, n2: int, inverse: bool, q):
     import torch
     import torch.distributed as dist
 
@@ -95,19 +98,19 @@ def dist_worker(rank: int, world: int, port: int, n1: int, n2: int, q):
         x = (rng.standard_normal(n1 * n2) + 1j * rng.standard_normal(n1 * n2)).astype(np.complex64)
         c2 = n2 // world
         cols = torch.from_numpy(np.ascontiguousarray(x.reshape(n1, n2)[:, rank * c2:(rank + 1) * c2]))
-        out = dist_fft(cols, n1, n2, fft_last_dim=_numpy_fft_last_dim)
+        out = dist_fft(cols, n1, n2, inverse=inverse, columns=cpu_columns)
         q.put((rank, out.numpy()))
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 4])
-def test_distributed_four_step_one_all_to_all(world):
+@pytest.mark.parametrize("world,inverse", [(2, False), (4, False), (2, True)])
+def test_distributed_four_step_one_all_to_all(world, inverse):
     n1, n2 = 64, 128
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = free_port()
-    procs = [ctx.Process(target=dist_worker, args=(r, world, port, n1, n2, q)) for r in range(world)]
+    procs = [ctx.Process(target=dist_worker, args=(r, world, port, n1, n2, inverse, q)) for r in range(world)]
     for p in procs:
         p.start()
     res = dict(q.get(timeout=120) for _ in range(world))
@@ -116,7 +119,8 @@ def test_distributed_four_step_one_all_to_all(world):
         assert p.exitcode == 0
     rng = np.random.default_rng(42)
     x = (rng.standard_normal(n1 * n2) + 1j * rng.standard_normal(n1 * n2)).astype(np.complex64)
-    want = np.fft.fft(x.astype(np.complex128))
+    z = x.astype(np.complex128)
+    want = np.fft.ifft(z) * z.size if inverse else np.fft.fft(z)
     r1 = n1 // world
     for rank, blk in res.items():
         # block element [k1 - rank r1][k2] = X[k1 + n1 k2]
@@ -124,6 +128,33 @@ def test_distributed_four_step_one_all_to_all(world):
         k2 = np.arange(n2)[None, :]
         ref = want[k1 + n1 * k2]
         assert np.linalg.norm(blk - ref) / np.linalg.norm(ref) < 1e-6
+
+
+def emulate_ranks(x, n1, n2, world, columns, inverse=False):
+    """The distributed four-step's data path with the exchange done by indexing, all ranks in one
+    process: returns the (n1, n2) array of row blocks, [k1][k2] = X[k1 + n1 k2]."""
+    c2, r1 = n2 // world, n1 // world
+    m = x.reshape(n1, n2)
+    sends = [columns(np.ascontiguousarray(m[:, r * c2:(r + 1) * c2]).reshape(-1), n1, c2, world, n1 * n2, r * c2,
+                     1 if inverse else 0).reshape(world, c2 * r1) for r in range(world)]
+    rows = []
+    for r in range(world):
+        recv = np.concatenate([sends[s][r] for s in range(world)])  # rank s's block for rank r
+        rows.append(columns(recv, n2, r1, 1, 0, 0, 2 if inverse else 0).reshape(r1, n2))
+    return np.concatenate(rows)
+
+
+@pytest.mark.parametrize("world,n1,n2", [(1, 16, 32), (2, 64, 32), (4, 32, 128), (8, 128, 64)])
+def test_column_contract_composes_to_the_transform(oracle, world, n1, n2):
+    """The two column-transform steps and the exchange, on the oracle's FP64 statement of the
+    column contract, give the n1 n2-point transform (forward and inverse)."""
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal(n1 * n2) + 1j * rng.standard_normal(n1 * n2)
+    for inverse in (False, True):
+        got = emulate_ranks(x, n1, n2, world, oracle.columns_fp64, inverse)
+        want = np.fft.ifft(x) * x.size if inverse else np.fft.fft(x)
+        ref = want.reshape(n2, n1).T  # [k1][k2] = X[k1 + n1 k2]
+        assert np.abs(got - ref).max() < 1e-9 * np.abs(ref).max()
 
 
 def test_shard_balance():
