@@ -372,6 +372,29 @@ def other_configs(torch, ofb, L, stream, peak):
         out[f"split-BF16 {batch} x 2^{lg}"] = rec
         fp.destroy()
         del x, y
+    # distributed four-step: one rank's two column-transform calls for N = 2^30 over 8 ranks
+    # (n1 = 2^12, n2 = 2^18: a 2^12 x 2^15 column block, 2^27 values, per rank)
+    P, n1, n2, rank = 8, 1 << 12, 1 << 18, 3
+    c2, r1 = n2 // P, n1 // P
+    s1 = ofb.Columns(n1, c2, P, n1 * n2, rank * c2)
+    s3 = ofb.Columns(n2, r1)
+    xb = torch.randn(n1 * c2, dtype=torch.complex64, device="cuda", generator=g)
+    yb, zb = torch.empty_like(xb), torch.empty_like(xb)
+    t1 = _time(torch, stream, lambda: s1.execute(xb.data_ptr(), yb.data_ptr(), 0, sptr))
+    t3 = _time(torch, stream, lambda: s3.execute(yb.data_ptr(), zb.data_ptr(), 0, sptr))
+    moved = 16.0 * n1 * c2  # bytes read + written per pass
+    exch = 8.0 * n1 * c2 * (P - 1) / P
+    out["distributed 2^30 over 8 ranks, one rank's local steps"] = {
+        "us_step1_columns_2^12_one_pass": 1e6 * t1, "us_step3_columns_2^18_two_passes": 1e6 * t3,
+        "us_local": 1e6 * (t1 + t3), "gbs_step1": moved / t1 / 1e9, "gbs_step3_per_pass": 2 * moved / t3 / 1e9,
+        "bytes_sent_per_rank": exch, "us_exchange_projected_at_770GBs": 1e6 * exch / 770e9,
+        "note": "measured on one GPU: one rank's two onefft_columns_execute calls (transforms, the 2^30-point "
+                "twiddle and the all-to-all layout inside the kernels); the NCCL all-to-all between them needs "
+                "8 GPUs and was not run, its time is projected from the 770 GB/s measured peer copy; "
+                "correctness in tests/test_gpu_distributed.py"}
+    s1.destroy()
+    s3.destroy()
+    del xb, yb, zb
     # differentiable layer: forward + backward of sum |W * FFT(x)|^2, batch 512 x 8192
     from onefft_b200 import torch_fft
     n, batch = 8192, 512

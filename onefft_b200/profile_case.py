@@ -8,6 +8,8 @@
     python -m onefft_b200.profile_case --log2n 16 --batch 256 --bf16x3    # split-BF16 tensor cores
     python -m onefft_b200.profile_case --log2n 24 --split 8,8,8 --cols 4,4,4 --tma --chunk 4 --fuse-lag 1
                                                                           # fused passes 0+1
+    python -m onefft_b200.profile_case --log2n 12 --columns 32768,8,30,3  # column transform:
+                               # n = 2^12, cols, blocks, log2 big_n, rank (col0 = rank cols: rank 3 of 2^30 / 8)
 
 Inputs are seeded standard-normal values on the device; the plan (and its table kernels) is
 built before the timed transforms, so `ncu -k regex:k_pass -s <n>` can skip to them.
@@ -38,8 +40,21 @@ def main():
     ap.add_argument("--fuse-lag", type=int, default=0, help="with --chunk and --tma: fused passes 0+1")
     ap.add_argument("--no-l2-keep", action="store_true", help="with --split: no L2 eviction hints")
     ap.add_argument("--uneven", type=int, default=0, help="run an uneven batch of this many transforms")
+    ap.add_argument("--columns", default="", help="cols,blocks,log2 big_n,rank: the column transform of "
+                                                  "an n x cols matrix with col0 = rank cols (onefft_columns_execute)")
     args = ap.parse_args()
     g = torch.Generator(device="cuda").manual_seed(7)
+    if args.columns:
+        cols, blocks, lbig, rank = (int(v) for v in args.columns.split(","))
+        n = 1 << args.log2n
+        c = ofb.Columns(n, cols, blocks, (1 << lbig) if lbig else 0, rank * cols)
+        x = torch.randn(n * cols, dtype=torch.complex64, device="cuda", generator=g)
+        y = torch.empty_like(x)
+        for _ in range(args.reps):
+            c.execute(x.data_ptr(), y.data_ptr(), ofb.SWAP_IN | ofb.SWAP_OUT if args.inverse else 0)
+        torch.cuda.synchronize()
+        print(f"columns n=2^{args.log2n} x {cols}, blocks {blocks}, big_n 2^{lbig}: {args.reps} runs")
+        return
     if args.uneven:
         rng = np.random.default_rng(7)
         log2n = rng.integers(4, 17, args.uneven).astype(np.int32)
