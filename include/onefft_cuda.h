@@ -220,6 +220,9 @@ ONEFFT_API void onefft_columns_destroy(onefft_columns *columns);
 #define ONEFFT_SWAP_OUT 2
 ONEFFT_API int onefft_columns_execute(const onefft_columns *columns, const float *d_in, float *d_out, int flags,
                                       void *stream);
+/* As onefft_plan_status, for a column transform: 0, or the error of a tile copy whose bounded
+ * wait ran out since the last call (reading clears it); call after synchronising the stream. */
+ONEFFT_API int onefft_columns_status(const onefft_columns *columns);
 
 /* ---- information and testing hooks -------------------------------------------------------------*/
 

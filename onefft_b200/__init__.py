@@ -38,7 +38,7 @@ C_SYMBOLS = (
     "onefft_uneven_create", "onefft_uneven_create_split", "onefft_uneven_destroy", "onefft_uneven_span", "onefft_uneven_execute",
     "onefft_uneven_status",
     "onefft_uneven_execute_noalloc",
-    "onefft_columns_create", "onefft_columns_destroy", "onefft_columns_execute",
+    "onefft_columns_create", "onefft_columns_destroy", "onefft_columns_execute", "onefft_columns_status",
     "onefft_last_error", "onefft_plan_status", "onefft_debug_fail_alloc", "onefft_debug_twiddles",
     "onefft_debug_launch_count", "onefft_debug_expire_waits",
 )
@@ -120,6 +120,8 @@ def lib() -> ctypes.CDLL:
     L.onefft_columns_destroy.restype = None
     L.onefft_columns_execute.argtypes = [_vp, _vp, _vp, ctypes.c_int, _vp]
     L.onefft_columns_execute.restype = ctypes.c_int
+    L.onefft_columns_status.argtypes = [_vp]
+    L.onefft_columns_status.restype = ctypes.c_int
     L.onefft_last_error.argtypes = []
     L.onefft_last_error.restype = ctypes.c_char_p
     L.onefft_debug_fail_alloc.argtypes = [ctypes.c_int]
@@ -394,6 +396,17 @@ class Columns:
         rc = lib().onefft_columns_execute(self._h, d_in, d_out, flags, stream)
         if rc != 0:
             raise RuntimeError(f"onefft_columns_execute failed ({rc}): {last_error()}")
+
+    def status(self) -> int:
+        """onefft_columns_status: 0, or the error code of a tile copy whose bounded wait ran out
+        since the last call (reading clears it); call after synchronising the stream."""
+        return int(lib().onefft_columns_status(self._h))
+
+    def check(self) -> None:
+        """Raises if a kernel of this column transform recorded a failure (see status())."""
+        rc = self.status()
+        if rc != 0:
+            raise RuntimeError(f"column transform failed on the device ({rc}): {last_error()}")
 
     def destroy(self) -> None:
         if getattr(self, "_h", None):

@@ -45,8 +45,8 @@ def tile_ok(l: int, c: int) -> bool:
 
 def tma_ok(l: int, c: int) -> bool:
     """Tile shapes with a bulk-tensor-copy kernel (fft_tma.cu, pass_tma_supported)."""
-    return 6 <= l <= 12 and 1 <= c <= 4 and l + c <= 13 and (l, c) in {
-        (12, 1), (11, 1), (11, 2), (10, 1), (10, 2), (10, 3), (9, 2), (9, 3), (9, 4), (8, 2), (8, 3), (8, 4),
+    return 6 <= l <= 12 and 1 <= c <= 4 and l + c <= 14 and (l, c) in {
+        (12, 2), (12, 1), (11, 1), (11, 2), (10, 1), (10, 2), (10, 3), (9, 2), (9, 3), (9, 4), (8, 2), (8, 3), (8, 4),
         (7, 3), (7, 4), (6, 4)}
 
 

@@ -89,6 +89,10 @@ cudaError_t launch_pass(int mode, int log_l, int log_c, const PassArgs& a, int b
 // the default tile width pass_log_c(log_l); one launch over the whole matrix of 2^a.log2n values
 // (log2n <= 31, at least one tile).
 cudaError_t launch_pass_columns(int mode, int log_l, const PassArgs& a, cudaStream_t stream);
+// The same through the bulk-tensor-copy tiles (fft_tma.cu): tile width column_tma_log_c(log_l)
+// (-1: none for this length); a.in 16-byte aligned; a.err set (an expired copy wait).
+int column_tma_log_c(int log_l);
+cudaError_t launch_pass_columns_tma(int mode, int log_l, const PassArgs& a, cudaStream_t stream);
 // TMA-staged passes (fft_tma.cu): same arithmetic as launch_pass; 16-byte aligned buffers,
 // batch <= 65535, shapes pass_tma_supported()
 bool pass_tma_supported(int log_l, int log_c);

@@ -162,6 +162,10 @@ __host__ __device__ constexpr int tma_smem_bytes(int log_l, int log_c) {
 // the tile is not run and tma_tile returns false), and issued() right after issuing it, so that
 // work which waits on memory overlaps the copy; every thread calls landed() once the copy has
 // landed, before the tile's arithmetic.
+// X: a pass of a column transform (PassArgs' column fields, as pass_tile): the first pass takes
+// its factor from the column fields and, with colstore, writes the column layout with plain
+// stores; the last pass reads its tile from `tin` (a.in, the work array) and writes the column
+// layout of a.out with plain stores instead of the bulk tensor store.
 struct NoHook {
     __device__ void operator()() const {}
 };
@@ -170,7 +174,7 @@ struct AlwaysReady {
 };
 
 template <int LOG_L, int LOG_C, int MODE, bool W, class Ready = AlwaysReady, class Issued = NoHook,
-          class Landed = NoHook>
+          class Landed = NoHook, bool X = false>
 __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* tin, const CUtensorMap* tout,
                                          unsigned t, int b, float2* smem, uint64_t* bar, unsigned parity, bool fresh,
                                          int tid, Ready ready = Ready(), Issued issued = Issued(),
@@ -206,7 +210,14 @@ __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* t
     // inter-pass twiddle factors (as pass_tile) while the copy is in flight
     float2* tws = smem + spad(C * L - 1) + 1;
     float2 wjf = make_float2(1.f, 0.f);
-    if (MODE != 2) {
+    bool twiddled = MODE != 2;
+    if constexpr (X) {
+        twiddled = MODE != 1 && a.tw_lo != nullptr;  // the same for the whole block
+        if (twiddled) {
+            column_twiddle_rows<LOG_L, LOG_C, MODE>(a, col0, tws, tid, C * T);
+            wjf = column_twiddle_lane<LOG_L, MODE>(a, col0, c, j);
+        }
+    } else if (MODE != 2) {
         pass_twiddle_rows<LOG_L, LOG_C, MODE>(a, col0, tws, tid, C * T);
         wjf = pass_twiddle_lane<LOG_L>(a, MODE == 0 ? col0 + c : (col0 >> a.log_s) << a.log_s, j);
     }
@@ -233,7 +244,7 @@ __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* t
     }
     __syncthreads();  // the dense tile is consumed; the exchanges reuse its memory
     tile_fft<LOG_L, C>(v, j, a.stw, smem, c);
-    if (MODE != 2) {
+    if (twiddled) {
         if (Stages<LOG_L>::COUNT == 1) __syncthreads();
         const float2* tw = tws + (MODE == 0 ? c * 17 : 0);
 #pragma unroll
@@ -249,6 +260,15 @@ __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* t
         __syncthreads();
         const int cc = tid >> (LOG_L - 4), kk0 = tid & (T - 1);
         const unsigned rr = col0 + cc;
+        if (X && a.colstore) {
+            const float2* r = smem + spad(kk0 * C + cc);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const float2 x = r[padc(i * T * C)];
+                a.out[column_dst(a, rr, (unsigned)(kk0 + i * T))] = a.swap_out ? swap_ri(x) : x;
+            }
+            return true;
+        }
         const unsigned j2 = rr & ((1u << a.rev_b2) - 1), j1 = rr >> a.rev_b2;
         float2* q = a.out + ((long long)b << a.log2n) + (((j1 + (j2 << a.rev_b1)) << LOG_L) + kk0);
         const float2* r = smem + spad(kk0 * C + cc);
@@ -259,6 +279,13 @@ __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* t
         } else {
 #pragma unroll
             for (int i = 0; i < 16; ++i) q[i * T] = r[padc(i * T * C)];
+        }
+    } else if (X && MODE == 2) {
+        const unsigned long long hh = (unsigned)h, q = (unsigned)(q0 + c);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const float2 x = a.swap_out ? swap_ri(v[k]) : v[k];
+            a.out[column_dst(a, hh, q + ((unsigned long long)(j + T * k) << a.log_s))] = x;
         }
     } else {
         // dense tile back in shared memory, then one bulk tensor store
@@ -284,8 +311,8 @@ __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* t
 }
 
 // One tile per block (blockIdx.x the tile, blockIdx.y the transform of the batch).
-template <int LOG_L, int LOG_C, int MODE, bool W>
-__global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_L, LOG_C, MODE>()))
+template <int LOG_L, int LOG_C, int MODE, bool W, bool X = false>
+__global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (X ? 0 : tma_min_blocks<LOG_L, LOG_C, MODE>()))
     k_pass_tma(PassArgs a, const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout) {
     extern __shared__ __align__(1024) float2 smem[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + tma_bar_offset(LOG_L, LOG_C));
@@ -293,7 +320,8 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (tma_min_blocks<LOG_
         if (threadIdx.x == 0) *(volatile unsigned*)a.err = 2u;
         return;
     }
-    tma_tile<LOG_L, LOG_C, MODE, W>(a, &tin, &tout, blockIdx.x, (int)blockIdx.y, smem, bar, 0u, true,
+    tma_tile<LOG_L, LOG_C, MODE, W, AlwaysReady, NoHook, NoHook, X>(a, &tin, &tout, blockIdx.x, (int)blockIdx.y, smem,
+                                                                    bar, 0u, true,
                                     (int)threadIdx.x);
 }
 
@@ -579,8 +607,10 @@ static cudaError_t launch_tma_w(const PassArgs& a, int batch, cudaStream_t strea
 }
 
 // Tile shapes with a TMA kernel (the only ones pass_tma_supported accepts): widths 2 .. 16
-// columns (16-byte minimum row segment), up to 8192 values per tile.
+// columns (16-byte minimum row segment), up to 8192 values per tile, and 4 columns of 4096
+// (16384 values, 1024 threads, one block per SM) for two-pass 2^24.
 #define OFB_TMA_SHAPES(X) \
+    X(12, 2)              \
     X(12, 1)              \
     X(11, 1)              \
     X(11, 2)              \
@@ -630,6 +660,58 @@ cudaError_t launch_pass_tma(int mode, int log_l, int log_c, const PassArgs& a, i
     case 1: return launch_tma_mode<1>(log_l, log_c, a, batch, stream);
     default: return launch_tma_mode<2>(log_l, log_c, a, batch, stream);
     }
+}
+
+// ---- column transforms through the bulk-tensor-copy tiles ----------------------------------------
+
+// Tile width (log2 columns) of a column-transform pass of length 2^log_l, -1: no TMA tile.
+int column_tma_log_c(int log_l) {
+    switch (log_l) {
+    case 12: return 1;
+    case 11: return 2;
+    case 10: return 3;
+    case 9: return 3;
+    case 8: return 3;
+    case 7: return 4;
+    case 6: return 4;
+    default: return -1;
+    }
+}
+
+// Both modes read their tile from a.in (first pass: the matrix; last pass: the work array in the
+// first pass's layout) and write a.out with plain stores.
+template <int LOG_L, int LOG_C, int MODE>
+static cudaError_t launch_columns_tma_t(const PassArgs& a, cudaStream_t stream) {
+    constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
+    constexpr int SMEM = tma_smem_bytes(LOG_L, LOG_C);
+    auto kernel = k_pass_tma<LOG_L, LOG_C, MODE, false, true>;
+    static std::atomic<unsigned long long> done{0};
+    const cudaError_t attr = smem_limit((const void*)kernel, SMEM, done);
+    if (attr != cudaSuccess) return attr;
+    if (a.log2n > 31 || a.log2n < LOG_L + LOG_C) return cudaErrorInvalidValue;
+    CUtensorMap tin;
+    if (!make_map(&tin, a.in, MODE, a.log2n, LOG_L, LOG_C, a.log_s, 1)) return cudaErrorInvalidValue;
+    PassArgs b = a;
+    b.tli = 31;
+    kernel<<<1u << (a.log2n - LOG_L - LOG_C), THREADS, SMEM, stream>>>(b, tin, tin);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pass_columns_tma(int mode, int log_l, const PassArgs& a, cudaStream_t stream) {
+    if (mode != 0 && mode != 2) return cudaErrorInvalidValue;
+#define OFB_COLUMNS_TMA_CASE(LL, LC) \
+    case LL: return mode == 0 ? launch_columns_tma_t<LL, LC, 0>(a, stream) : launch_columns_tma_t<LL, LC, 2>(a, stream);
+    switch (log_l) {
+        OFB_COLUMNS_TMA_CASE(12, 1)
+        OFB_COLUMNS_TMA_CASE(11, 2)
+        OFB_COLUMNS_TMA_CASE(10, 3)
+        OFB_COLUMNS_TMA_CASE(9, 3)
+        OFB_COLUMNS_TMA_CASE(8, 3)
+        OFB_COLUMNS_TMA_CASE(7, 4)
+        OFB_COLUMNS_TMA_CASE(6, 4)
+    default: return cudaErrorInvalidValue;
+    }
+#undef OFB_COLUMNS_TMA_CASE
 }
 
 }  // namespace ofb

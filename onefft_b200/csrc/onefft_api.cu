@@ -1251,6 +1251,7 @@ struct onefft_columns {
     const double2 *big_lo = nullptr, *big_hi = nullptr;  // w_N (big_n > 0)
     int big_lo_bits = 0;
     float2 *work = nullptr;
+    unsigned *err_host = nullptr, *err = nullptr;  // mapped pinned error word (TMA copy waits)
 };
 
 static bool pow2_log(unsigned long long x, int *l) {
@@ -1340,8 +1341,15 @@ extern "C" onefft_columns *onefft_columns_create(size_t n, size_t cols, size_t b
         return nullptr;
     }
     char *base = (char *)c->mem;
+    e = cudaHostAlloc((void **)&c->err_host, sizeof(unsigned), cudaHostAllocMapped | cudaHostAllocPortable);
+    if (e == cudaSuccess) {
+        *(volatile unsigned *)c->err_host = 0;
+        e = cudaHostGetDevicePointer((void **)&c->err, c->err_host, 0);
+    } else {
+        c->err_host = nullptr;
+    }
     cudaStream_t s = nullptr;
-    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
     if (e == cudaSuccess) {
         for (int i = 0; i < c->npass && e == cudaSuccess; ++i) {
             c->stw[i] = (const float2 *)(base + off[i]);
@@ -1364,6 +1372,7 @@ extern "C" onefft_columns *onefft_columns_create(size_t n, size_t cols, size_t b
     }
     if (e != cudaSuccess) {
         cudaFree(c->mem);
+        if (c->err_host) cudaFreeHost(c->err_host);
         delete c;
         cuda_error(e, "column transform table build");
         return nullptr;
@@ -1377,8 +1386,20 @@ extern "C" void onefft_columns_destroy(onefft_columns *c) {
     cudaGetDevice(&cur);
     if (cur != c->device) cudaSetDevice(c->device);
     cudaFree(c->mem);
+    if (c->err_host) cudaFreeHost(c->err_host);
     if (cur >= 0 && cur != c->device) cudaSetDevice(cur);
     delete c;
+}
+
+extern "C" int onefft_columns_status(const onefft_columns *c) {
+    t_last_error.clear();
+    if (!c) return set_error(ONEFFT_ERR_ARG, "NULL column transform");
+    if (!c->err_host) return 0;
+    volatile unsigned *word = c->err_host;
+    const unsigned flag = *word;
+    if (!flag) return 0;
+    *word = 0;
+    return set_error(ONEFFT_ERR_CUDA_BASE, "a bulk tensor copy did not complete in time (code %u)", flag);
 }
 
 extern "C" int onefft_columns_execute(const onefft_columns *c, const float *d_in, float *d_out, int flags,
@@ -1391,9 +1412,18 @@ extern "C" int onefft_columns_execute(const onefft_columns *c, const float *d_in
     const size_t bytes = sizeof(float2) << (c->m + c->lb);
     if (ranges_overlap(d_in, d_out, bytes)) return set_error(ONEFFT_ERR_ARG, "input and output overlap");
     const cudaStream_t s = (cudaStream_t)stream;
+    // a pass runs through its bulk-tensor-copy tile when its length has one and what it reads is
+    // 16-byte aligned (the work array always is)
+    const bool in16 = ((uintptr_t)d_in & 15) == 0;
+    auto run = [&](int mode, int len, const PassArgs &x, bool aligned) {
+        g_launches.fetch_add(1);
+        if (aligned && column_tma_log_c(len) >= 0) return launch_pass_columns_tma(mode, len, x, s);
+        return launch_pass_columns(mode, len, x, s);
+    };
     PassArgs a{};
     a.log2n = c->m + c->lb;
     a.tli = 31;
+    a.err = c->err;
     a.swap_in = (flags & ONEFFT_SWAP_IN) ? 1 : 0;
     a.xlog_blk = c->log_blk;
     a.xlog_cols = c->lb;
@@ -1410,8 +1440,7 @@ extern "C" int onefft_columns_execute(const onefft_columns *c, const float *d_in
         a.xlog2n = c->log2big;
         a.xcol0 = c->col0;
         a.colstore = 1;
-        g_launches.fetch_add(1);
-        e = launch_pass_columns(0, c->len[0], a, s);
+        e = run(0, c->len[0], a, in16);
     } else {
         PassArgs p0 = a;
         p0.in = (const float2 *)d_in;
@@ -1425,8 +1454,7 @@ extern "C" int onefft_columns_execute(const onefft_columns *c, const float *d_in
         p0.lo_bits = c->lo_bits;
         p0.xlog2n = c->m;
         p0.tw_shift = c->lb;
-        g_launches.fetch_add(1);
-        e = launch_pass_columns(0, c->len[0], p0, s);
+        e = run(0, c->len[0], p0, in16);
         if (e == cudaSuccess) {
             PassArgs p1 = a;
             p1.in = c->work;
@@ -1441,8 +1469,7 @@ extern "C" int onefft_columns_execute(const onefft_columns *c, const float *d_in
             p1.xlog2n = c->log2big;
             p1.xcol0 = c->col0;
             p1.colstore = 1;
-            g_launches.fetch_add(1);
-            e = launch_pass_columns(2, c->len[1], p1, s);
+            e = run(2, c->len[1], p1, true);
         }
     }
     return e == cudaSuccess ? 0 : cuda_error(e, "column transform launch");

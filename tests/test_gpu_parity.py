@@ -210,6 +210,7 @@ SHAPES = [  # (n, split, tile widths, chunk)
 TMA_SHAPES = [  # (n, split, tile widths, chunk) run through the bulk-tensor-copy kernels
     (1 << 12, (6, 6), (4, 4), 0), (1 << 16, (8, 8), (2, 3), 0), (1 << 18, (9, 9), (4, 3), 0),
     (1 << 20, (10, 10), (1, 2), 0), (1 << 22, (11, 11), (2, 1), 0), (1 << 24, (12, 12), (1, 1), 0),
+    (1 << 24, (12, 12), (2, 2), 0), (1 << 20, (12, 8), (2, 3), 0),
     (1 << 21, (7, 7, 7), (4, 3, 4), 5), (1 << 24, (8, 8, 8), (4, 4, 4), 0), (1 << 23, (9, 7, 7), (3, 4, 3), 0),
 ]
 
