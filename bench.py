@@ -29,12 +29,18 @@ With --impl reference only rank 0 runs: it times the reference CPU library on th
 with all host threads and prints the same metric with "impl": "reference". Multi-GPU (torchrun,
 one process per GPU): every rank runs the whole workload on its own data (weak scaling, no
 collective on the data path).
+
+With --dist the step is instead ONE forward transform of 2^27 N values distributed over the N
+ranks (2^27 per rank): each rank's column transform writes the all-to-all send layout, NCCL's
+all_to_all_single exchanges the blocks, and a second column transform gives the rank's rows of
+the result (onefft_b200/distributed.py); same timing rules, metric 5 N log2 N per step.
 """
 from __future__ import annotations
 
 import argparse
 import concurrent.futures
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -76,6 +82,9 @@ def parse():
     ap.add_argument("--e2e-schedule", default="pairs", choices=["pairs", "chains"],
                     help="host threads of the end-to-end measurement (see the e2e section)")
     ap.add_argument("--e2e-chains", type=int, default=2, help="chains per item of --e2e-schedule chains")
+    ap.add_argument("--dist", action="store_true",
+                    help="instead of the benchmark step: ONE forward transform of 2^27 N values distributed over "
+                         "the N ranks (distributed four-step: column transform, NCCL all-to-all, column transform)")
     return ap.parse_args()
 
 
@@ -422,6 +431,77 @@ def other_configs(torch, ofb, L, stream, peak):
     return out
 
 
+def run_dist(args, world: int, rank: int, local_rank: int):
+    """One transform of N = 2^27 world values over the ranks (weak scaling: 2^27 values, 1 GiB, per
+    rank): n1 = 2^12 rows, n2 = N / 2^12 columns; per step each rank runs its column transform into
+    the all-to-all send layout, the all-to-all, and the column transform of what it received
+    (onefft_b200.distributed.dist_fft). Timed on the device with CUDA events, max over ranks."""
+    import datetime
+
+    import torch
+
+    import onefft_b200 as ofb
+    from onefft_b200.distributed import clear_cache, gpu_columns
+    from onefft_b200.shard import max_over_ranks
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    n1 = 1 << 12
+    n2 = (1 << 15) * world
+    c2, r1 = n2 // world, n1 // world
+    g = torch.Generator(device="cuda").manual_seed(77 + rank)
+    x = torch.randn(n1 * c2, dtype=torch.complex64, device="cuda", generator=g)
+    recv = torch.empty_like(x)
+    L = ofb.lib()
+
+    def step():
+        send = gpu_columns(x, n1, c2, world, n1 * n2, rank * c2, 0)
+        if dist:
+            dist.all_to_all_single(recv, send)
+            src = recv
+        else:
+            src = send
+        return gpu_columns(src, n2, r1, 1, 0, 0, 0)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    launches0 = L.onefft_debug_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = int(L.onefft_debug_launch_count() - launches0)
+    clk = clocks.stop()
+    t = max_over_ranks(e0.elapsed_time(e1) / 1e3, device="cuda") / args.steps
+    N = n1 * n2
+    clear_cache()
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        line = {"metric": "distributed transform GFLOP/s (5 N log2 N per step)", "value": 5.0 * N * math.log2(N) / t / 1e9,
+                "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"one forward transform of 2^{int(math.log2(N))} values over {world} GPUs, "
+                                       f"n1 = 2^12, n2 = 2^{int(math.log2(n2))}",
+                           "inputs": "larger than L2", "parallelism": f"four-step, one all-to-all, {world} ranks"},
+                "gpu_launches": launches, "clocks": clk, "mode": "dist"}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -429,6 +509,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.dist:
+        run_dist(args, world, rank, local_rank)
         return
 
     import torch

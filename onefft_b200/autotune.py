@@ -50,6 +50,11 @@ def tma_ok(l: int, c: int) -> bool:
         (7, 3), (7, 4), (6, 4)}
 
 
+def pass_log_c_default(log_l: int) -> int:
+    """The library's default tile width of a pass (pass_log_c in fft_kernels.cu)."""
+    return 4 if log_l <= 9 else 3 if log_l == 10 else 2
+
+
 def candidates(m: int):
     """(log2 lengths, log2 tile widths, log2 chunk) shapes worth timing for 2^m."""
     out = []
@@ -304,6 +309,9 @@ def main():
     ap.add_argument("--uneven", action="store_true", help="tune the uneven batch's in-block splits instead")
     ap.add_argument("--batched", action="store_true", help="tune the transforms per block of sizes 2^4 .. 2^14")
     ap.add_argument("--fused", action="store_true", help="tune the fused first two passes of three-pass sizes")
+    ap.add_argument("--split", default="", help="time only this split (log2 lengths, e.g. 12,12) against the "
+                                                 "default plan, with --cols tile widths (e.g. 2,2)")
+    ap.add_argument("--cols", default="")
     args = ap.parse_args()
     if args.fused:
         res = tune_fused(max(args.min, 22), args.max, args.reps)
@@ -331,6 +339,10 @@ def main():
         best = None
         rows = []
         cands = candidates(m)[: args.max_candidates]
+        if args.split:
+            ls = tuple(int(v) for v in args.split.split(","))
+            cs = tuple(int(v) for v in args.cols.split(",")) if args.cols else tuple(pass_log_c_default(l) for l in ls)
+            cands = [(ls, cs, 0)]
         variants = [(ls, cs, g, keep, tma) for ls, cs, g in cands for keep in (True, False)
                     for tma in ((False, True) if any(tma_ok(l, c) for l, c in zip(ls, cs)) else (False,))]
         if args.tma_only:
