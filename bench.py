@@ -382,8 +382,10 @@ def other_configs(torch, ofb, L, stream, peak):
         fp.destroy()
         del x, y
     # distributed four-step: one rank's two column-transform calls for N = 2^30 over 8 ranks
-    # (n1 = 2^12, n2 = 2^18: a 2^12 x 2^15 column block, 2^27 values, per rank)
-    P, n1, n2, rank = 8, 1 << 12, 1 << 18, 3
+    # (n1 = 2^10, n2 = 2^20: a 2^10 x 2^17 column block, 2^27 values, per rank; n1 = 2^10 keeps
+    # step 1 to one pass of 1024-value tiles of 8 columns, which run near the copy bound, where
+    # 4096-value columns would run their one pass at ~60 % of it)
+    P, n1, n2, rank = 8, 1 << 10, 1 << 20, 3
     c2, r1 = n2 // P, n1 // P
     s1 = ofb.Columns(n1, c2, P, n1 * n2, rank * c2)
     s3 = ofb.Columns(n2, r1)
@@ -394,7 +396,7 @@ def other_configs(torch, ofb, L, stream, peak):
     moved = 16.0 * n1 * c2  # bytes read + written per pass
     exch = 8.0 * n1 * c2 * (P - 1) / P
     out["distributed 2^30 over 8 ranks, one rank's local steps"] = {
-        "us_step1_columns_2^12_one_pass": 1e6 * t1, "us_step3_columns_2^18_two_passes": 1e6 * t3,
+        "us_step1_columns_2^10_one_pass": 1e6 * t1, "us_step3_columns_2^20_two_passes": 1e6 * t3,
         "us_local": 1e6 * (t1 + t3), "gbs_step1": moved / t1 / 1e9, "gbs_step3_per_pass": 2 * moved / t3 / 1e9,
         "bytes_sent_per_rank": exch, "us_exchange_projected_at_770GBs": 1e6 * exch / 770e9,
         "note": "measured on one GPU: one rank's two onefft_columns_execute calls (transforms, the 2^30-point "
@@ -433,7 +435,7 @@ def other_configs(torch, ofb, L, stream, peak):
 
 def run_dist(args, world: int, rank: int, local_rank: int):
     """One transform of N = 2^27 world values over the ranks (weak scaling: 2^27 values, 1 GiB, per
-    rank): n1 = 2^12 rows, n2 = N / 2^12 columns; per step each rank runs its column transform into
+    rank): n1 = 2^10 rows, n2 = N / 2^10 columns; per step each rank runs its column transform into
     the all-to-all send layout, the all-to-all, and the column transform of what it received
     (onefft_b200.distributed.dist_fft). Timed on the device with CUDA events, max over ranks."""
     import datetime
@@ -450,8 +452,10 @@ def run_dist(args, world: int, rank: int, local_rank: int):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
-    n1 = 1 << 12
-    n2 = (1 << 15) * world
+    n1 = 1 << 10
+    n2 = (1 << 17) * world
+    if n1 // world < 16 or n2 > 1 << 24:
+        raise SystemExit("--dist supports 1 .. 64 ranks")
     c2, r1 = n2 // world, n1 // world
     g = torch.Generator(device="cuda").manual_seed(77 + rank)
     x = torch.randn(n1 * c2, dtype=torch.complex64, device="cuda", generator=g)
@@ -496,7 +500,7 @@ def run_dist(args, world: int, rank: int, local_rank: int):
                 "ms_per_step": 1e3 * t, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic",
                 "config": {"workload": f"one forward transform of 2^{int(math.log2(N))} values over {world} GPUs, "
-                                       f"n1 = 2^12, n2 = 2^{int(math.log2(n2))}",
+                                       f"n1 = 2^10, n2 = 2^{int(math.log2(n2))}",
                            "inputs": "larger than L2", "parallelism": f"four-step, one all-to-all, {world} ranks"},
                 "gpu_launches": launches, "clocks": clk, "mode": "dist"}
         print(json.dumps(line), flush=True)
