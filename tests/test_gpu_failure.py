@@ -57,3 +57,33 @@ def test_expired_wait_reported_and_recovered(ofb, oracle):
     assert plan.status() == 0
     assert np.array_equal(d_out.cpu().numpy(), y)
     plan.destroy()
+
+
+@pytest.mark.parametrize("ln", [10, 20])
+def test_column_transform_expired_wait_reported(ofb, oracle, ln):
+    """The column transform's tile copies (one pass at 2^10, two at 2^20) take the same failure
+    path: nothing written, onefft_columns_status() reports it once, the next call is correct."""
+    import torch
+    L = ofb.lib()
+    n, cols = 1 << ln, 64
+    c = ofb.Columns(n, cols, 4, n * 256, 3 * cols)
+    x = torch.from_numpy(oracle.gen_normal(2 * n * cols, 0xC01).view(np.complex64)).cuda()
+    y = torch.full_like(x, 7.0)
+    s = torch.cuda.current_stream().cuda_stream
+    assert L.onefft_debug_expire_waits(1) == 0
+    try:
+        c.execute(x.data_ptr(), y.data_ptr(), 0, s)
+        torch.cuda.synchronize()
+    finally:
+        assert L.onefft_debug_expire_waits(0) == 0
+    assert (y == 7.0).all(), "output written after a failed column transform"
+    assert c.status() == ERR_CUDA_BASE
+    assert "did not complete" in ofb.last_error()
+    assert c.status() == 0
+    c.execute(x.data_ptr(), y.data_ptr(), 0, s)
+    torch.cuda.synchronize()
+    assert c.status() == 0
+    want = oracle.columns_fp64(x.cpu().numpy(), n, cols, 4, n * 256, 3 * cols)
+    got = y.cpu().numpy()
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) < oracle.tolerance(ln + 8)
+    c.destroy()
