@@ -1411,6 +1411,10 @@ extern "C" int onefft_columns_execute(const onefft_columns *c, const float *d_in
     if (flags & ~(ONEFFT_SWAP_IN | ONEFFT_SWAP_OUT)) return set_error(ONEFFT_ERR_ARG, "unknown flags %d", flags);
     const size_t bytes = sizeof(float2) << (c->m + c->lb);
     if (ranges_overlap(d_in, d_out, bytes)) return set_error(ONEFFT_ERR_ARG, "input and output overlap");
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || cur != c->device)
+        return set_error(ONEFFT_ERR_ARG, "the column transform belongs to device %d, the current device is %d",
+                         c->device, cur);
     const cudaStream_t s = (cudaStream_t)stream;
     // a pass runs through its bulk-tensor-copy tile when its length has one and what it reads is
     // 16-byte aligned (the work array always is)
