@@ -92,9 +92,10 @@ def ofb_pass_log_c(log_l: int) -> int:
 
 
 @pytest.mark.parametrize("world,n1,n2", [(4, 1 << 10, 1 << 12), (8, 1 << 13, 1 << 12), (2, 1 << 14, 1 << 11)])
-def test_distributed_ranks_emulated_on_gpu(ofb, oracle, world, n1, n2):
+def test_distributed_ranks_emulated_on_gpu(ofb, oracle, ref_errors, world, n1, n2):
     """P ranks' column transforms on this library's kernels, run one after another, with the
-    exchange done by indexing: the n1 n2-point transform in both directions."""
+    exchange done by indexing: the n1 n2-point transform in both directions, within the parity
+    rule (at most 2x the reference library's rel-RMS on normal inputs of the same size)."""
     import torch
 
     from onefft_b200.distributed import clear_cache, gpu_columns
@@ -112,6 +113,9 @@ def test_distributed_ranks_emulated_on_gpu(ofb, oracle, world, n1, n2):
         print(f"distributed four-step, {world} ranks emulated, n=2^{n.bit_length() - 1} "
               f"{'inverse' if inverse else 'forward'}: rel RMS {err:.3g}")
         assert err < oracle.tolerance(n.bit_length() - 1)
+        ref = ref_errors["normal"].get(str(n.bit_length() - 1))
+        if ref:
+            assert err <= 2 * ref["inverse" if inverse else "forward"]["rel_rms"]
     clear_cache()
 
 
