@@ -34,9 +34,9 @@ __device__ __forceinline__ double2 zpow(double2 w, unsigned e) {
 
 // Inter-pass twiddles of a pass tile: output j + T kk of a column with factor F (first pass:
 // the column index; middle pass: S h) is multiplied by w_n^(F j) * w_n^(F T kk), each factor
-// rounded once to FP32. The 16 factors w_n^(F T kk) of a column are FP64 powers of one table
-// product w_n^(F T), so a tile reads the tables at C addresses for them instead of once per
-// factor; they go to shared memory (rows of 17). Each thread reads its w_n^(F j) directly.
+// rounded once to FP32. Both factors are powers of ONE table product per column (w_n^F and
+// w_n^(F T)), so a tile reads the FP64 tables at C addresses instead of once per factor.
+// The 16 factors w_n^(F T kk) of each column go to shared memory (rows of 17).
 template <int LOG_L, int LOG_C, int MODE>
 __device__ __forceinline__ void pass_twiddle_rows(const PassArgs& a, unsigned col0, float2* tws, int tid, int nthreads) {
     constexpr unsigned T = 1u << (LOG_L - 4);
@@ -49,11 +49,10 @@ __device__ __forceinline__ void pass_twiddle_rows(const PassArgs& a, unsigned co
         tws[cc * 17 + kk] = make_float2((float)w.x, (float)w.y);
     }
 }
-// ... and the thread's own factor w_n^(F j), one product of two table entries (F j < n: the
-// first pass's F is below n / L and j below L / 16; a middle pass's F j T stays below n).
+// ... and the thread's own factor w_n^(F j).
 template <int LOG_L>
 __device__ __forceinline__ float2 pass_twiddle_lane(const PassArgs& a, unsigned f, int j) {
-    const double2 w = big_twiddle_f64(a.tw_lo, a.tw_hi, a.lo_bits, f * (unsigned)j);
+    const double2 w = zpow<LOG_L - 4>(big_twiddle_f64(a.tw_lo, a.tw_hi, a.lo_bits, f), (unsigned)j);
     return make_float2((float)w.x, (float)w.y);
 }
 
@@ -65,8 +64,7 @@ __device__ __forceinline__ double2 wide_twiddle_f64(const PassArgs& a, unsigned 
 }
 // The factors of a column-transform tile, split like the inter-pass twiddles above (one FP32
 // rounding per factor). First pass: output j + T kk of column col gets w_N^(F (j + T kk)),
-// F = xcol0 + (col >> tw_shift): rows w_N^(F T kk) per column, lane w_N^(F j) (a table product,
-// like pass_twiddle_lane). Last pass: output
+// F = xcol0 + (col >> tw_shift): rows w_N^(F T kk) per column, lane w_N^(F j). Last pass: output
 // k = q + 2^log_s (j + T kk) of transform h = col >> log_s (q = col mod 2^log_s) gets
 // w_N^((xcol0 + h) k): rows w_N^((xcol0 + h) 2^log_s T kk), one per tile (a tile's columns share
 // h), lane w_N^((xcol0 + h)(q + 2^log_s j)).
@@ -86,7 +84,7 @@ template <int LOG_L, int MODE>
 __device__ __forceinline__ float2 column_twiddle_lane(const PassArgs& a, unsigned col0, int c, int j) {
     double2 w;
     if (MODE == 0) {
-        w = wide_twiddle_f64(a, (a.xcol0 + ((col0 + c) >> a.tw_shift)) * (unsigned long long)j);
+        w = zpow<LOG_L - 4>(wide_twiddle_f64(a, a.xcol0 + ((col0 + c) >> a.tw_shift)), (unsigned)j);
     } else {
         const unsigned long long f = a.xcol0 + (col0 >> a.log_s);
         const unsigned long long q = (col0 & ((1u << a.log_s) - 1)) + c;
