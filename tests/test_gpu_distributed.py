@@ -135,3 +135,27 @@ def test_dist_fft_single_rank_on_gpu(ofb, oracle):
         print(f"distributed four-step on one rank, n=2^23 {'inverse' if inverse else 'forward'}: rel RMS {err:.3g}")
         assert err < oracle.tolerance(23)
     clear_cache()
+
+
+@pytest.mark.parametrize("ln", [10, 16])
+def test_columns_misaligned_input_same_bits(ofb, ln):
+    """An input 8 bytes off a 16-byte boundary takes the per-thread-load kernel for the first pass
+    instead of the bulk tensor copy: the same bits."""
+    import torch
+
+    from onefft_b200 import Columns
+    n, cols = 1 << ln, 32
+    c = Columns(n, cols, 4, n * 64, 5 * cols)
+    g = torch.Generator(device="cuda").manual_seed(ln)
+    buf = torch.randn(n * cols + 1, dtype=torch.complex64, device="cuda", generator=g)
+    x_odd = buf[1:]  # 8 bytes past the allocation's 256-byte boundary
+    x_even = x_odd.clone()
+    assert x_odd.data_ptr() % 16 == 8 and x_even.data_ptr() % 16 == 0
+    a, b = torch.empty_like(x_even), torch.empty_like(x_even)
+    s = torch.cuda.current_stream().cuda_stream
+    c.execute(x_even.data_ptr(), a.data_ptr(), 0, s)
+    c.execute(x_odd.data_ptr(), b.data_ptr(), 0, s)
+    torch.cuda.synchronize()
+    c.check()
+    c.destroy()
+    assert torch.equal(a, b)
