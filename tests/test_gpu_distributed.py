@@ -145,7 +145,7 @@ def test_columns_misaligned_input_same_bits(ofb, ln):
 
     from onefft_b200 import Columns
     n, cols = 1 << ln, 32
-    c = Columns(n, cols, 4, n * 64, 5 * cols)
+    c = Columns(n, cols, 4, n * 256, 5 * cols)
     g = torch.Generator(device="cuda").manual_seed(ln)
     buf = torch.randn(n * cols + 1, dtype=torch.complex64, device="cuda", generator=g)
     x_odd = buf[1:]  # 8 bytes past the allocation's 256-byte boundary
