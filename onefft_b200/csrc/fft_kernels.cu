@@ -66,27 +66,31 @@ __global__ void k_twiddle_probe(float2* __restrict__ dst, unsigned log2n, unsign
 // ---- kernels --------------------------------------------------------------------------------------
 
 // W: the pointwise weights pre / post are applied (instantiated only for weighted calls).
-// One transform per thread, 256 per block. The block's transforms are one contiguous run, loaded
-// and stored with consecutive threads on consecutive values through shared memory (padded one
-// slot per 16, so each thread's n values, n * 8 bytes apart from its neighbour's, sit in distinct
-// banks): loading each thread's own n values directly touched 32 lines per warp instruction, and
-// an n = 8 batch of 2^26 values took 324 us (ncu, 39 % of DRAM bandwidth, load/store throttled).
-// Same arithmetic as tiny_transform, so the same bits.
+// Each thread transforms the 8 / n consecutive transforms of 8 consecutive values, so a block
+// covers 2048 values. The block's transforms are one contiguous run, loaded and stored with
+// consecutive threads on consecutive values through shared memory (padded one slot per 16, so
+// each thread's 8 values, 64 bytes from its neighbour's, sit in distinct banks). Loading each
+// thread's own values directly touched 32 lines per warp instruction: an n = 8 batch of 2^26
+// values took 324 us (ncu, 39 % of DRAM bandwidth, load/store throttled). Same arithmetic as
+// tiny_transform, so the same bits.
+constexpr int kTinyValues = 2048;  // values per block
 template <int LOG_N, bool W>
 __global__ void __launch_bounds__(256) k_tiny(const float2* __restrict__ in, float2* __restrict__ out,
                                               long long batch, int inverse, const float2* __restrict__ pre,
                                               const float2* __restrict__ post) {
-    constexpr int N = 1 << LOG_N;
-    __shared__ float2 s[256 * N + (256 * N >> 4)];
-    const long long first = (long long)blockIdx.x * 256;
-    const int count = batch - first < 256 ? (int)(batch - first) : 256;
+    constexpr int N = 1 << LOG_N, PER = 8 >> LOG_N, PB = kTinyValues >> LOG_N;  // per thread, per block
+    __shared__ float2 s[kTinyValues + (kTinyValues >> 4)];
+    const long long first = (long long)blockIdx.x * PB;
+    const int count = batch - first < PB ? (int)(batch - first) : PB;
     const int total = count << LOG_N;
     const float2* src = in + (first << LOG_N);
     float2* dst = out + (first << LOG_N);
     for (int i = threadIdx.x; i < total; i += 256) s[spad(i)] = __ldg(src + i);
     __syncthreads();
-    const int t = threadIdx.x;
-    if (t < count) {
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+        const int t = threadIdx.x * PER + p;
+        if (t >= count) break;
         float2 a[N];
 #pragma unroll
         for (int i = 0; i < N; ++i) {
@@ -234,12 +238,13 @@ template <int LOG_N>
 static cudaError_t launch_tiny_t(const float2* in, float2* out, long long batch, int inverse, cudaStream_t stream,
                                  const float2* pre, const float2* post) {
     const bool w = pre || post;
-    long long blocks = (batch + 255) / 256;
+    constexpr long long PB = kTinyValues >> LOG_N;  // transforms per block
+    long long blocks = (batch + PB - 1) / PB;
     while (blocks > 0) {
         long long now = blocks < 0x7fffffffll ? blocks : 0x7fffffffll;
         if (w) k_tiny<LOG_N, true><<<(unsigned)now, 256, 0, stream>>>(in, out, batch, inverse, pre, post);
         else k_tiny<LOG_N, false><<<(unsigned)now, 256, 0, stream>>>(in, out, batch, inverse, nullptr, nullptr);
-        long long done = now * 256;
+        long long done = now * PB;
         in += done << LOG_N;
         out += done << LOG_N;
         batch -= done;
