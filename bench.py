@@ -446,12 +446,22 @@ def run_dist(args, world: int, rank: int, local_rank: int):
     from onefft_b200.distributed import clear_cache, gpu_columns
     from onefft_b200.shard import max_over_ranks
 
+    import socket
+
+    import torch.distributed as dist
+
     torch.cuda.set_device(local_rank)
-    dist = None
+    # the exchange always runs through NCCL: under torchrun over the job's ranks, alone as a
+    # one-rank group (NCCL's all-to-all copying the blocks to this GPU itself)
     if world > 1:
-        import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
+    else:
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                                timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
     n1 = 1 << 10
     n2 = (1 << 17) * world
     if n1 // world < 16 or n2 > 1 << 24:
@@ -464,18 +474,13 @@ def run_dist(args, world: int, rank: int, local_rank: int):
 
     def step():
         send = gpu_columns(x, n1, c2, world, n1 * n2, rank * c2, 0)
-        if dist:
-            dist.all_to_all_single(recv, send)
-            src = recv
-        else:
-            src = send
-        return gpu_columns(src, n2, r1, 1, 0, 0, 0)
+        dist.all_to_all_single(recv, send)
+        return gpu_columns(recv, n2, r1, 1, 0, 0, 0)
 
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    dist.barrier()
     clocks = ClockSampler(local_rank)
     clocks.start()
     launches0 = L.onefft_debug_launch_count()
@@ -485,15 +490,13 @@ def run_dist(args, world: int, rank: int, local_rank: int):
         step()
     e1.record()
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    dist.barrier()
     launches = int(L.onefft_debug_launch_count() - launches0)
     clk = clocks.stop()
     t = max_over_ranks(e0.elapsed_time(e1) / 1e3, device="cuda") / args.steps
     N = n1 * n2
     clear_cache()
-    if dist:
-        dist.destroy_process_group()
+    dist.destroy_process_group()
     if rank == 0:
         line = {"metric": "distributed transform GFLOP/s (5 N log2 N per step)", "value": 5.0 * N * math.log2(N) / t / 1e9,
                 "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,

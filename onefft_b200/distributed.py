@@ -62,8 +62,9 @@ def dist_fft(x_cols: torch.Tensor, n1: int, n2: int, group=None, inverse: bool =
     block of the result. columns(x, n, cols, blocks, big_n, col0, flags): the column transform
     (default gpu_columns, this library's kernels)."""
     import torch.distributed as dist
-    world = dist.get_world_size(group) if group is not None or dist.is_initialized() else 1
-    rank = dist.get_rank(group) if world > 1 else 0
+    grouped = group is not None or (dist.is_available() and dist.is_initialized())
+    world = dist.get_world_size(group) if grouped else 1
+    rank = dist.get_rank(group) if grouped else 0
     if n1 % world or n2 % world:
         raise ValueError("N1 and N2 must be multiples of the number of ranks")
     c2, r1 = n2 // world, n1 // world
@@ -72,8 +73,9 @@ def dist_fft(x_cols: torch.Tensor, n1: int, n2: int, group=None, inverse: bool =
     col = columns if columns is not None else gpu_columns
     # 1. n1-point transforms down the columns, twiddle w_n^(j2 k1), send layout [s][j2 local][k1 local]
     send = col(x_cols.reshape(-1), n1, c2, world, n1 * n2, rank * c2, SWAP_IN if inverse else 0)
-    # 2. one all-to-all: block s goes to rank s
-    if world > 1:
+    # 2. one all-to-all: block s goes to rank s (through the process group whenever there is one,
+    # a one-rank group included)
+    if grouped:
         recv = torch.empty_like(send)
         dist.all_to_all_single(recv, send, group=group)
     else:

@@ -159,3 +159,31 @@ def test_columns_misaligned_input_same_bits(ofb, ln):
     c.check()
     c.destroy()
     assert torch.equal(a, b)
+
+
+def test_dist_fft_through_nccl_one_rank(ofb, oracle):
+    """dist_fft with an NCCL process group of one rank: the exchange runs through NCCL's
+    all_to_all on the GPU (a copy to itself), the result is the transform."""
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    from onefft_b200.distributed import clear_cache, dist_fft
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            device_id=torch.device("cuda", 0))
+    try:
+        n1, n2 = 1024, 2048
+        x = oracle.gen_normal(2 * n1 * n2, 0xCC1).view(np.complex64)
+        cols = torch.from_numpy(x.reshape(n1, n2).copy()).cuda()
+        out = dist_fft(cols, n1, n2).cpu().numpy()
+        torch.cuda.synchronize()
+    finally:
+        dist.destroy_process_group()
+        clear_cache()
+    got = np.ascontiguousarray(out.T).reshape(-1)
+    want = oracle.fft64_numpy(x.view(np.float32))
+    assert oracle.rel_rms(got.view(np.float32), want) < oracle.tolerance(21)
