@@ -215,7 +215,11 @@ ONEFFT_API onefft_columns *onefft_columns_create(size_t n, size_t cols, size_t b
 ONEFFT_API void onefft_columns_destroy(onefft_columns *columns);
 /* flags: ONEFFT_SWAP_IN exchanges re/im of the input as it is read, ONEFFT_SWAP_OUT of the
  * result as it is written (after the twiddle). d_in / d_out: n cols complex values each, 8-byte
- * aligned device pointers, not overlapping. Enqueue only, like the other device entry points. */
+ * aligned device pointers, not overlapping (16-byte aligned input lets the first pass stage its
+ * tiles by bulk tensor copies; the results are the same bits either way). Enqueue only, like the
+ * other device entry points. For n > 2^12 the object's work buffer holds the values between the
+ * two passes: calls on one object whose GPU work overlaps (other streams, other threads) race on
+ * it, so issue them in order on one stream or give each stream its own object. */
 #define ONEFFT_SWAP_IN 1
 #define ONEFFT_SWAP_OUT 2
 ONEFFT_API int onefft_columns_execute(const onefft_columns *columns, const float *d_in, float *d_out, int flags,

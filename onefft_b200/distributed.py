@@ -33,7 +33,8 @@ def gpu_columns(x: torch.Tensor, n: int, cols: int, blocks: int, big_n: int, col
     """The column transform of the n x cols matrix x (complex64 on a CUDA device) on the current
     stream: returns the n * cols results in the column layout of onefft_columns_execute. The
     column-transform objects (tables and, for n > 2^12, an n * cols work buffer) are kept per
-    shape; clear_cache() frees them."""
+    device and shape, so calls with the same shape must not run concurrently on different streams
+    (they would share the work buffer); clear_cache() frees them."""
     from . import Columns
     if x.dtype != torch.complex64 or not x.is_contiguous():
         raise ValueError("expected a contiguous complex64 tensor")
