@@ -8,7 +8,10 @@ Rows, each forward and inverse:
     2^0 .. 2^20, through the drop-in host call onefft_plan_forward / _inverse;
   - standard normal inputs at 2^10, 2^12, 2^13, 2^16, 2^20, 2^22, 2^24 .. 2^27 (the batched
     configuration's single sizes), through the device-pointer calls;
-  - the 16384 x 4096 batch (standard normal): the worst of 64 sampled transforms.
+  - the 16384 x 4096 batch (standard normal): the worst of 64 sampled transforms;
+  - the distributed four-step (onefft_b200/distributed.py) on the standard normal inputs of 2^22,
+    2^24, 2^25 and 2^27, its P ranks' column transforms run one after another on this GPU with
+    the all-to-all done by indexing (the same exchange the multi-rank tests run through gloo).
 Columns: relative RMS against FP64 (tests/test_onefft.c:64-71) of this library and of the
 reference (tests/golden/ref_errors.json, the reference library run on the same inputs), their
 ratio (the parity rule asks <= 2), and the max-abs error of each.
@@ -73,6 +76,29 @@ def main(out_path: str) -> None:
         del d_in, d_out
         plan.destroy()
         print("normal", l, flush=True)
+    # the distributed four-step: (log2 n, ranks, log2 n1)
+    from test_multigpu_gloo import emulate_ranks
+
+    from onefft_b200.distributed import clear_cache, gpu_columns
+
+    def columns(v, n, cols, blocks, big_n, col0, flags):
+        t = torch.from_numpy(np.ascontiguousarray(v, np.complex64)).cuda()
+        return gpu_columns(t, n, cols, blocks, big_n, col0, flags).cpu().numpy()
+
+    for l, world, l1 in ((22, 4, 10), (24, 8, 10), (25, 8, 12), (27, 8, 10)):
+        n = 1 << l
+        x = O.gen_normal(2 * n, ref["seed_normal"] + l)
+        n1, n2 = 1 << l1, n >> l1
+        for inv in (0, 1):
+            d = "inverse" if inv else "forward"
+            blocks = emulate_ranks(x.view(np.complex64), n1, n2, world, columns, bool(inv))  # [k1][k2]
+            got = np.ascontiguousarray(blocks.T).reshape(-1).view(np.float32)  # natural order
+            del blocks
+            add(f"normal, distributed over {world} ranks (n1 = 2^{l1})", l, d, got, O.fft64_numpy(x, bool(inv)),
+                ref["normal"][str(l)][d])
+            del got
+        clear_cache()
+        print("distributed", l, flush=True)
     # the 16384 x 4096 batch: worst ratio over 64 sampled transforms
     n, batch = 4096, 16384
     x = O.gen_normal(2 * n * batch, 0xC0F2)
