@@ -131,7 +131,7 @@ struct Shape {
     int l2_keep;
     int chunk;
     int tma;
-    int fuse_lag;
+    int fuse_lag = 0;  // the tuned table leaves it out: no size runs the fused passes by default
 };
 
 // Fastest shapes measured on a B200 by onefft_b200/autotune.py (forward transform, L2 flushed
