@@ -100,11 +100,6 @@ ONEFFT_API onefft_plan *onefft_plan_create_split(size_t n, int npass, const int 
  * transform per block that brings the next transform in by one bulk copy while computing the
  * current one (for 16-byte aligned buffers; results equal the other widths bit for bit). */
 #define ONEFFT_COLS_PIPELINED 15
-/* npass = 1 at n = 2^13 or 2^14, log2_cols[0] = ONEFFT_COLS_SPLIT: each transform runs as 2 / 4
- * blocks of the 4096-point tile after one radix-2 / radix-4 decimation-in-frequency step (block h
- * computes the outputs h, h + R, h + 2R, ...). Within the FP32 error bound, not the bits of the
- * other widths; weighted calls on such a plan run the default kernel. */
-#define ONEFFT_COLS_SPLIT 16
 #define ONEFFT_OPT_L2_KEEP 1
 #define ONEFFT_OPT_TMA 2
 /* ONEFFT_OPT_FUSED (three passes, log2_chunk > 0, with ONEFFT_OPT_TMA): the first two passes run

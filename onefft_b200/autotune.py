@@ -188,9 +188,6 @@ def time_plan(plan, x, y, reps: int, flush) -> float:
 
 # ONEFFT_COLS_PIPELINED: the persistent double-buffered one-kernel form of 2^12 and 2^13
 PIPELINED = 15
-# ONEFFT_COLS_SPLIT: 2^13 / 2^14 as 2 / 4 blocks of the 4096-point tile per transform after one
-# decimation-in-frequency step (other bits than the default: compared within the FP32 tolerance)
-SPLIT = 16
 
 
 def batched_log_c_candidates(l: int) -> list[int]:
@@ -199,7 +196,7 @@ def batched_log_c_candidates(l: int) -> list[int]:
     and 2^13 also the pipelined form (fft_tma.cu, batched_pipe_supported)."""
     b = max(0, 12 - l)
     out = [c for c in (b - 1, b, b + 1) if c == b or (c >= 0 and l + c <= 13)]
-    return out + ([PIPELINED] if l in (12, 13) else []) + ([SPLIT] if l in (13, 14) else [])
+    return out + ([PIPELINED] if l in (12, 13) else [])
 
 
 def tune_batched(reps: int = 9) -> dict:
@@ -224,11 +221,7 @@ def tune_batched(reps: int = 9) -> dict:
             y.fill_(float("nan"))
             plan.dev_forward(x.data_ptr(), y.data_ptr(), batch)
             torch.cuda.synchronize()
-            if c == SPLIT:
-                err = ((y - ref).norm() / ref.norm()).item()
-                if err > 1e-6:
-                    raise RuntimeError(f"2^{l} split into 4096-point tiles differs from the default ({err:.2e})")
-            elif not torch.equal(y, ref):
+            if not torch.equal(y, ref):
                 raise RuntimeError(f"2^{l} with 2^{c} transforms per block differs from the default")
             ts = []
             for r in range(reps + 2):
@@ -245,7 +238,7 @@ def tune_batched(reps: int = 9) -> dict:
             times[c] = ts[len(ts) // 2]
         best = min(times, key=times.get)
         out[l] = {"log_c": best, "us": times}
-        label = lambda c: "pipelined" if c == PIPELINED else "split" if c == SPLIT else f"{1 << c}/block"  # noqa: E731
+        label = lambda c: "pipelined" if c == PIPELINED else f"{1 << c}/block"  # noqa: E731
         print(f"batched 2^{l} x {batch}: " + ", ".join(f"{label(c)} {t:.1f} us" for c, t in times.items()) +
               f" -> {label(best)}", flush=True)
         del x, ref, y

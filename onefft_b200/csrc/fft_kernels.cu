@@ -177,73 +177,6 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4))
     }
 }
 
-// n = 2^(12 + LOG_R) (2^13, 2^14) as R = 2^LOG_R blocks of the 4096-point tile per transform:
-// one radix-R decimation-in-frequency step on load, then block h computes
-//   X[R k + h] = FFT_4096(a_h)[k],   a_h[e] = w_n^(h e) sum_p x[e + 4096 p] w_R^(h p)
-// (n = e + 4096 p, k' = R k + h: w_n^(n k') = w_4096^(e k) w_n^(e h) w_R^(p h)). Each block reads
-// the whole transform (the R blocks of a transform run side by side, so the second and later
-// reads come from L2) and writes every R-th output; a block is the 256-thread, 32 KiB tile of the
-// one-kernel 2^12 path, so an SM holds four of them where it held one or two whole 2^13 / 2^14
-// transforms. dtw: w_n^k for k < (R - 1) 4096, FP32 rounded once; stw: the 2^12 stage table.
-template <int LOG_R, int INV>
-__global__ void __launch_bounds__(256) k_batched_dif(const float2* __restrict__ in, float2* __restrict__ out,
-                                                     const float2* __restrict__ stw, const float2* __restrict__ dtw) {
-    constexpr int R = 1 << LOG_R, M = 12 + LOG_R, Q = 4096, T = 256;
-    __shared__ float2 smem[Q + Q / 16];
-    const long long t = (long long)(blockIdx.x >> LOG_R);
-    const int h = (int)(blockIdx.x & (R - 1));
-    const float2* src = in + (t << M);
-    float2* dst = out + (t << M);
-    const int j = threadIdx.x;
-    float2 v[16];
-#pragma unroll
-    for (int kk = 0; kk < 16; ++kk) {
-        const int e = j + T * kk;
-        float2 x[R];
-#pragma unroll
-        for (int p = 0; p < R; ++p) {
-            const float2 y = ld_stream(src + e + Q * p);
-            x[p] = INV ? swap_ri(y) : y;
-        }
-        float2 a;
-        if constexpr (R == 2) {
-            a = h ? csub(x[0], x[1]) : cadd(x[0], x[1]);
-        } else {
-            const float2 s02 = cadd(x[0], x[2]), d02 = csub(x[0], x[2]);
-            const float2 s13 = cadd(x[1], x[3]), d13 = mul_mi(csub(x[1], x[3]));
-            a = h == 0 ? cadd(s02, s13) : h == 1 ? cadd(d02, d13) : h == 2 ? csub(s02, s13) : csub(d02, d13);
-        }
-        if (h) a = cmul(a, __ldg(dtw + h * e));
-        v[kk] = a;
-    }
-    tile_fft<12, 1>(v, j, stw, smem, 0);
-#pragma unroll
-    for (int kk = 0; kk < 16; ++kk) dst[R * (j + T * kk) + h] = INV ? swap_ri(v[kk]) : v[kk];
-}
-
-bool batched_dif_supported(int log2n) { return log2n == 13 || log2n == 14; }
-
-cudaError_t launch_batched_dif(int log2n, const float2* in, float2* out, long long batch, const float2* stw12,
-                               const float2* dtw, int inverse, cudaStream_t stream) {
-    if (!batched_dif_supported(log2n)) return cudaErrorInvalidValue;
-    const int lr = log2n - 12;
-    while (batch > 0) {
-        const long long now = batch < (0x7fffffffll >> lr) ? batch : (0x7fffffffll >> lr);
-        const unsigned grid = (unsigned)(now << lr);
-        if (lr == 1) {
-            if (inverse) k_batched_dif<1, 1><<<grid, 256, 0, stream>>>(in, out, stw12, dtw);
-            else k_batched_dif<1, 0><<<grid, 256, 0, stream>>>(in, out, stw12, dtw);
-        } else {
-            if (inverse) k_batched_dif<2, 1><<<grid, 256, 0, stream>>>(in, out, stw12, dtw);
-            else k_batched_dif<2, 0><<<grid, 256, 0, stream>>>(in, out, stw12, dtw);
-        }
-        in += now << log2n;
-        out += now << log2n;
-        batch -= now;
-    }
-    return cudaGetLastError();
-}
-
 template <int LOG_L, int LOG_C, int MODE, bool W, bool X = false>
 __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4)) k_pass(PassArgs a) {
     extern __shared__ float2 smem[];

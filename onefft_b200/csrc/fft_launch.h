@@ -112,12 +112,6 @@ bool pass01_fused_supported(int l0, int c0, int l1, int c1);
 bool batched_pipe_supported(int log2n);
 cudaError_t launch_batched_pipe(int log2n, const float2* in, float2* out, long long batch, const float2* stw,
                                 int inverse, unsigned* err, cudaStream_t stream);
-// One-kernel sizes 2^13 / 2^14 as 2 / 4 blocks of the 4096-point tile per transform after one
-// radix-2 / radix-4 decimation-in-frequency step (fft_kernels.cu, k_batched_dif). stw12: the
-// stage table of 2^12; dtw: w_n^k for k < (R - 1) 4096 (FP32). Not the bits of k_batched.
-bool batched_dif_supported(int log2n);
-cudaError_t launch_batched_dif(int log2n, const float2* in, float2* out, long long batch, const float2* stw12,
-                               const float2* dtw, int inverse, cudaStream_t stream);
 cudaError_t launch_pass01_fused(int l0, int c0, int l1, int c1, const PassArgs& a0, const PassArgs& a1, int g,
                                 int len2, int lag, unsigned* ctr, cudaStream_t stream);
 cudaError_t launch_pass_tma(int mode, int log_l, int log_c, const PassArgs& a, int batch, cudaStream_t stream);

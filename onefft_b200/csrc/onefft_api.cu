@@ -116,8 +116,6 @@ struct onefft_plan {
     void *mem;             // the one device allocation
     size_t mem_bytes;
     const float2 *stw[3];  // stage twiddles of each pass's length
-    const float2 *stw12;   // one kernel as 4096-point tiles (kDifCols): the 2^12 stage table
-    const float2 *dtw;     // ... and w_n^k for k < (2^(log2n - 12) - 1) 4096
     const double2 *tw_lo;  // two-level FP64 tables of w_n (npass >= 2)
     const double2 *tw_hi;
     int lo_bits;
@@ -185,16 +183,12 @@ static Shape tuned_shape(int m) {
 // One kernel, cols[0] = this: the persistent pipelined kernel (launch_batched_pipe) instead of
 // k_batched (ONEFFT_COLS_PIPELINED in onefft_cuda.h).
 constexpr int kPipelinedCols = 15;
-// One kernel, cols[0] = this: 2^13 / 2^14 as 2 / 4 blocks of the 4096-point tile per transform
-// after one decimation-in-frequency step (launch_batched_dif; ONEFFT_COLS_SPLIT in onefft_cuda.h).
-constexpr int kDifCols = 16;
 
 static bool valid_shape(int m, const Shape &s) {
     if (s.npass == 1)
         return s.len[0] == m && m <= kMaxSingleLog2 &&
                (s.cols[0] == -1 || batched_log_c_supported(m, s.cols[0]) ||
-                (s.cols[0] == kPipelinedCols && batched_pipe_supported(m)) ||
-               (s.cols[0] == kDifCols && batched_dif_supported(m)));
+                (s.cols[0] == kPipelinedCols && batched_pipe_supported(m)));
     if (s.npass < 2 || s.npass > 3) return false;
     int sum = 0;
     for (int p = 0; p < s.npass; ++p) {
@@ -244,15 +238,6 @@ static onefft_plan *plan_build(size_t n, int m, const Shape &shape) {
         off[i] = bytes;
         bytes = align256(bytes + sizeof(float2) * (size_t)stage_table_entries_host(p->len[i]));
     }
-    const bool dif = p->npass == 1 && p->cols[0] == kDifCols;
-    size_t stw12_off = 0, dtw_off = 0, dtw_count = 0;
-    if (dif) {
-        stw12_off = bytes;
-        bytes = align256(bytes + sizeof(float2) * (size_t)stage_table_entries_host(12));
-        dtw_count = (((size_t)1 << (m - 12)) - 1) << 12;
-        dtw_off = bytes;
-        bytes = align256(bytes + sizeof(float2) * dtw_count);
-    }
     size_t lo_off = bytes, hi_off = bytes;
     if (p->npass >= 2) {
         p->lo_bits = m / 2;
@@ -299,12 +284,6 @@ static onefft_plan *plan_build(size_t n, int m, const Shape &shape) {
         for (int i = 0; i < p->npass && e == cudaSuccess; ++i) {
             p->stw[i] = (const float2 *)(base + off[i]);
             e = launch_stage_table((float2 *)(base + off[i]), p->len[i], s);
-        }
-        if (dif && e == cudaSuccess) {
-            p->stw12 = (const float2 *)(base + stw12_off);
-            p->dtw = (const float2 *)(base + dtw_off);
-            e = launch_stage_table((float2 *)p->stw12, 12, s);
-            if (e == cudaSuccess) e = launch_twiddle_probe((float2 *)p->dtw, (unsigned)m, dtw_count, s);
         }
         if (p->npass >= 2 && e == cudaSuccess) {
             p->tw_lo = (const double2 *)(base + lo_off);
@@ -465,11 +444,6 @@ static cudaError_t plan_enqueue(const onefft_plan *p, const float2 *in, float2 *
     if (p->npass == 1) {
         g_launches.fetch_add(1);
         if (p->tc) return launch_single_kernel_tc(p->log2n, in, out, batch, p->stw[0], inverse, p->tc, s);
-        if (p->cols[0] == kDifCols) {
-            // the weighted kernels are k_batched's (the stage table of n is in the plan too)
-            if (!pre && !post) return launch_batched_dif(p->log2n, in, out, batch, p->stw12, p->dtw, inverse, s);
-            return launch_single_kernel(p->log2n, in, out, batch, p->stw[0], inverse, s, pre, post, -1);
-        }
         if (p->cols[0] == kPipelinedCols) {
             // bulk copies need 16-byte aligned transforms; weighted calls use k_batched's weights
             if (!pre && !post && !((uintptr_t)in & 15))

@@ -289,9 +289,8 @@ def test_device_batched_equals_single_bitwise(ofb, oracle, log2n, batch):
 def test_transforms_per_block_same_bits(ofb, oracle, log2n):
     """Every compiled number of transforms per block of a one-kernel size (the autotuner's
     choices) gives the default plan's results bit for bit, both directions, with a batch that
-    leaves the last block partly empty; invalid widths are rejected. (The split form of 2^13 /
-    2^14, another decomposition, has its own test below.)"""
-    from onefft_b200.autotune import SPLIT, batched_log_c_candidates
+    leaves the last block partly empty; invalid widths are rejected."""
+    from onefft_b200.autotune import batched_log_c_candidates
     torch = _torch()
     n = 1 << log2n
     batch = 2 * (1 << max(0, 13 - log2n)) + 3
@@ -302,8 +301,6 @@ def test_transforms_per_block_same_bits(ofb, oracle, log2n):
     for inv in (False, True):
         (default.dev_inverse if inv else default.dev_forward)(d_in.data_ptr(), want.data_ptr(), batch)
         for c in batched_log_c_candidates(log2n):
-            if c == SPLIT:
-                continue
             plan = ofb.Plan(n, split=(log2n,), cols=(c,))
             got = torch.full_like(d_in, float("nan"))
             (plan.dev_inverse if inv else plan.dev_forward)(d_in.data_ptr(), got.data_ptr(), batch)
@@ -415,43 +412,3 @@ def test_pipelined_one_kernel_equals_default(ofb, log2n, batch):
             assert T.equal(a, b), (log2n, batch, off, inv)
     pipe.destroy()
     ref.destroy()
-
-
-@pytest.mark.parametrize("log2n", [13, 14])
-def test_split_one_kernel_form(ofb, oracle, ref_errors, log2n):
-    """ONEFFT_COLS_SPLIT: 2^13 / 2^14 as 2 / 4 blocks of the 4096-point tile after one
-    decimation-in-frequency step. Against FP64 within the tolerance and, where the reference's
-    error on the same input is recorded, at most 2x it; a batch's transform b equals the same
-    transform alone bit for bit; weighted calls on such a plan run the default kernel."""
-    torch = _torch()
-    n = 1 << log2n
-    plan = ofb.Plan(n, split=(log2n,), cols=(16,))
-    x = oracle.gen_normal(2 * n, ref_errors["seed_normal"] + log2n)
-    ref = ref_errors["normal"].get(str(log2n))
-    for inv in (False, True):
-        got = plan.inverse(x) if inv else plan.forward(x)
-        err = oracle.rel_rms(got, oracle.fft64_numpy(x, inv))
-        assert err < oracle.tolerance(log2n), (log2n, inv, err)
-        if ref:
-            assert err <= 2 * ref["inverse" if inv else "forward"]["rel_rms"], (log2n, inv, err)
-    batch = 37
-    xb = oracle.gen_normal(2 * n * batch, 91 + log2n)
-    d = torch.from_numpy(xb).cuda()
-    whole, one = torch.empty_like(d), torch.empty_like(d[:2 * n])
-    for inv in (False, True):
-        (plan.dev_inverse if inv else plan.dev_forward)(d.data_ptr(), whole.data_ptr(), batch)
-        for b in (0, 17, 36):
-            src = d[2 * n * b:2 * n * (b + 1)].clone()
-            (plan.dev_inverse if inv else plan.dev_forward)(src.data_ptr(), one.data_ptr(), 1)
-            torch.cuda.synchronize()
-            assert torch.equal(one, whole[2 * n * b:2 * n * (b + 1)]), (log2n, inv, b)
-    ones = torch.zeros(2 * n, device="cuda")
-    ones[0::2] = 1.0
-    default = ofb.Plan(n)
-    a, b_ = torch.empty_like(d), torch.empty_like(d)
-    plan.dev_weighted(d.data_ptr(), a.data_ptr(), batch, pre=ones.data_ptr())
-    default.dev_weighted(d.data_ptr(), b_.data_ptr(), batch, pre=ones.data_ptr())
-    torch.cuda.synchronize()
-    assert torch.equal(a, b_)
-    default.destroy()
-    plan.destroy()
