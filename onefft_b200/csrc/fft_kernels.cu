@@ -1,6 +1,7 @@
 // The transform kernels for sm_100a and their launchers.
 //
-//   k_tiny     n = 1, 2, 4, 8: one thread per transform, all in registers.
+//   k_tiny     n = 1, 2, 4, 8: 8 / n transforms per thread in registers, 2048 values per block
+//              loaded and stored coalesced through shared memory.
 //   k_batched  n = 16 .. 2^14 in one kernel: each block holds C whole transforms (by default
 //              max(1, 4096 / n), or half or twice that as the plan's tuned width says; C n / 16
 //              threads, 16 values per thread), Stockham radix-16 stages in registers with
