@@ -594,9 +594,7 @@ static cudaError_t launch_tma_w(const PassArgs& a, int batch, cudaStream_t strea
     constexpr int SMEM = tma_smem_bytes(LOG_L, LOG_C);
     // the direction is compiled in where it matters: the first pass's loads, the last pass's stores
     const bool inverse = MODE == 0 ? a.swap_in != 0 : MODE == 2 ? a.swap_out != 0 : false;
-    // (the middle pass keeps the run-time form: compiled without the select its register
-    // allocation spilled, 56 bytes at 2^9 x 8 columns, and 2^27 went from 1.06 to 1.12 ms)
-    auto kernel = k_pass_tma<LOG_L, LOG_C, MODE, W, false, MODE == 1 ? -1 : 0>;
+    auto kernel = k_pass_tma<LOG_L, LOG_C, MODE, W, false, 0>;
     if constexpr (MODE != 1) {
         if (inverse) kernel = k_pass_tma<LOG_L, LOG_C, MODE, W, false, 1>;
     }
