@@ -173,11 +173,8 @@ struct AlwaysReady {
     __device__ bool operator()() const { return true; }
 };
 
-// SW: the direction as a compile-time constant (0 forward, 1 inverse: the first pass exchanges
-// re/im on load, the last on store), which saves two selects per value; -1 reads a.swap_in /
-// a.swap_out at run time.
 template <int LOG_L, int LOG_C, int MODE, bool W, class Ready = AlwaysReady, class Issued = NoHook,
-          class Landed = NoHook, bool X = false, int SW = -1>
+          class Landed = NoHook, bool X = false>
 __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* tin, const CUtensorMap* tout,
                                          unsigned t, int b, float2* smem, uint64_t* bar, unsigned parity, bool fresh,
                                          int tid, Ready ready = Ready(), Issued issued = Issued(),
@@ -243,7 +240,7 @@ __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* t
         if constexpr (W && MODE == 0) {
             if (a.pre) x = cmul(x, __ldg(a.pre + col0 + c + ((unsigned)(j + T * k) << a.log_s)));
         }
-        v[k] = (SW < 0 ? a.swap_in != 0 : (MODE == 0 && SW == 1)) ? swap_ri(x) : x;
+        v[k] = a.swap_in ? swap_ri(x) : x;
     }
     __syncthreads();  // the dense tile is consumed; the exchanges reuse its memory
     tile_fft<LOG_L, C>(v, j, a.stw, smem, c);
@@ -294,7 +291,7 @@ __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* t
         // dense tile back in shared memory, then one bulk tensor store
 #pragma unroll
         for (int k = 0; k < 16; ++k) {
-            float2 x = (SW < 0 ? a.swap_out != 0 : (MODE == 2 && SW == 1)) ? swap_ri(v[k]) : v[k];
+            float2 x = a.swap_out ? swap_ri(v[k]) : v[k];
             // output element q0 + c + (j + T k) S + h L S of the transform, natural order (last pass)
             if constexpr (W && MODE == 2) {
                 if (a.post)
@@ -314,7 +311,7 @@ __device__ __forceinline__ bool tma_tile(const PassArgs& a, const CUtensorMap* t
 }
 
 // One tile per block (blockIdx.x the tile, blockIdx.y the transform of the batch).
-template <int LOG_L, int LOG_C, int MODE, bool W, bool X = false, int SW = -1>
+template <int LOG_L, int LOG_C, int MODE, bool W, bool X = false>
 __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (X ? 0 : tma_min_blocks<LOG_L, LOG_C, MODE>()))
     k_pass_tma(PassArgs a, const __grid_constant__ CUtensorMap tin, const __grid_constant__ CUtensorMap tout) {
     extern __shared__ __align__(1024) float2 smem[];
@@ -323,7 +320,7 @@ __global__ void __launch_bounds__(1 << (LOG_L + LOG_C - 4), (X ? 0 : tma_min_blo
         if (threadIdx.x == 0) *(volatile unsigned*)a.err = 2u;
         return;
     }
-    tma_tile<LOG_L, LOG_C, MODE, W, AlwaysReady, NoHook, NoHook, X, SW>(a, &tin, &tout, blockIdx.x, (int)blockIdx.y, smem,
+    tma_tile<LOG_L, LOG_C, MODE, W, AlwaysReady, NoHook, NoHook, X>(a, &tin, &tout, blockIdx.x, (int)blockIdx.y, smem,
                                                                     bar, 0u, true,
                                     (int)threadIdx.x);
 }
@@ -592,14 +589,9 @@ template <int LOG_L, int LOG_C, int MODE, bool W>
 static cudaError_t launch_tma_w(const PassArgs& a, int batch, cudaStream_t stream) {
     constexpr int THREADS = 1 << (LOG_L + LOG_C - 4);
     constexpr int SMEM = tma_smem_bytes(LOG_L, LOG_C);
-    // the direction is compiled in where it matters: the first pass's loads, the last pass's stores
-    const bool inverse = MODE == 0 ? a.swap_in != 0 : MODE == 2 ? a.swap_out != 0 : false;
-    auto kernel = k_pass_tma<LOG_L, LOG_C, MODE, W, false, 0>;
-    if constexpr (MODE != 1) {
-        if (inverse) kernel = k_pass_tma<LOG_L, LOG_C, MODE, W, false, 1>;
-    }
-    static std::atomic<unsigned long long> done_fwd{0}, done_inv{0};
-    const cudaError_t attr = smem_limit((const void*)kernel, SMEM, inverse ? done_inv : done_fwd);
+    auto kernel = k_pass_tma<LOG_L, LOG_C, MODE, W>;
+    static std::atomic<unsigned long long> done{0};
+    const cudaError_t attr = smem_limit((const void*)kernel, SMEM, done);
     if (attr != cudaSuccess) return attr;
     // MODE 0 loads from `in` and stores with plain coalesced stores (tout unused); MODE 1/2
     // load and store the same tile of `out`
