@@ -222,6 +222,44 @@ def run_reference(args, rank: int):
 # ---- GPU side ------------------------------------------------------------------------------------
 
 
+def pcie_ceiling(torch, nbytes: int = 1 << 30) -> dict:
+    """Host <-> device copy bandwidth of this GPU with pinned buffers, as context for the end-to-end
+    number: one direction alone, and both at once on two streams (what a step of host calls can
+    reach at best). GB/s, best of three."""
+    h_up = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    h_down = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    d_up = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    d_down = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def timed(fn):
+        best = float("inf")
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            best = min(best, time.perf_counter() - t0)
+        return best
+
+    def up():
+        with torch.cuda.stream(s1):
+            d_up.copy_(h_up, non_blocking=True)
+
+    def down():
+        with torch.cuda.stream(s2):
+            h_down.copy_(d_down, non_blocking=True)
+
+    def both():
+        up()
+        down()
+
+    t_up, t_down, t_both = timed(up), timed(down), timed(both)
+    del h_up, h_down, d_up, d_down
+    return {"h2d_gbs": nbytes / t_up / 1e9, "d2h_gbs": nbytes / t_down / 1e9, "both_ways_gbs": 2 * nbytes / t_both / 1e9,
+            "note": "1 GiB pinned copies, best of 3; a step moves h2d_bytes_per_step each way"}
+
+
 def _time(torch, stream, fn, reps: int = 5, warm: int = 2) -> float:
     """Average seconds of fn() on the device (CUDA events on `stream`)."""
     for _ in range(warm):
@@ -727,7 +765,9 @@ def main():
                    torch.equal((hz[0] if isinstance(hz, list) else hz)[:4096].cuda(), w["z"][:4096])
                    for w, hx, hy, hz in host)
         nbytes = sum(2 * 8 * (1 << w["log2n"]) * w["batch"] for w in work)
+        link = pcie_ceiling(torch)
         e2e = {"value": world * STEP_FLOPS / t_e2e / 1e9, "unit": "GFLOP/s", "h2d_bytes_per_step": nbytes,
+               "link": link, "ms_per_step_at_link_ceiling": 1e3 * 2 * nbytes / (link["both_ways_gbs"] * 1e9),
                "d2h_bytes_per_step": nbytes, "ms_per_step": 1e3 * t_e2e, "steps": e2e_steps,
                "matches_device_path": bool(same),
                "calls": "onefft_plan_forward/_inverse (single) and onefft_plan_forward/_inverse_batched (batch), "
