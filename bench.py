@@ -79,7 +79,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-configs", action="store_true")
-    ap.add_argument("--e2e-schedule", default="pairs", choices=["pairs", "chains"],
+    ap.add_argument("--e2e-schedule", default="pairs", choices=["pairs", "offset", "chains"],
                     help="host threads of the end-to-end measurement (see the e2e section)")
     ap.add_argument("--e2e-chains", type=int, default=2, help="chains per item of --e2e-schedule chains")
     ap.add_argument("--dist", action="store_true",
@@ -690,20 +690,27 @@ def main():
             else:
                 (L.onefft_plan_inverse if inverse else L.onefft_plan_forward)(h, src.data_ptr(), dst.data_ptr())
 
+        offset = args.e2e_schedule == "offset"
+
         def e2e_steps_run(k):
             futs = []
             for (w, hx, hy, hz), (pf, pi) in zip(host, pools):
                 done_f = [threading.Event() for _ in range(k)]
                 done_i = [threading.Event() for _ in range(k)]
                 failed = []
+                nb = len(hy)
+                # "offset": the inverse thread starts half a call late (one copy of the item at
+                # ~55 GB/s), so its uploads meet the forward thread's downloads and the other way
+                # round; it stays behind because each of its calls starts when its previous ends
+                half = 8.0 * (1 << w["log2n"]) * w["batch"] / 55e9 if offset else 0.0
 
-                def fwd_thread(w=w, hx=hx, hy=hy, done_f=done_f, done_i=done_i, failed=failed):
+                def fwd_thread(w=w, hx=hx, hy=hy, done_f=done_f, done_i=done_i, failed=failed, nb=nb):
                     try:
                         for s in range(k):
-                            if s >= 2:
-                                done_i[s - 2].wait()
+                            if s >= nb:
+                                done_i[s - nb].wait()
                             if not failed:
-                                call(w, hx, hy[s & 1], False)
+                                call(w, hx, hy[s % nb], False)
                             done_f[s].set()
                     except BaseException:
                         failed.append(1)
@@ -711,12 +718,14 @@ def main():
                             e.set()
                         raise
 
-                def inv_thread(w=w, hy=hy, hz=hz, done_f=done_f, done_i=done_i, failed=failed):
+                def inv_thread(w=w, hy=hy, hz=hz, done_f=done_f, done_i=done_i, failed=failed, nb=nb, half=half):
                     try:
                         for s in range(k):
                             done_f[s].wait()
+                            if s == 0 and half:
+                                time.sleep(half)
                             if not failed:
-                                call(w, hy[s & 1], hz, True)
+                                call(w, hy[s % nb], hz, True)
                             done_i[s].set()
                     except BaseException:
                         failed.append(1)
@@ -747,6 +756,9 @@ def main():
             for f in futs:
                 f.result()
 
+        if offset:  # three intermediates: forward s waits only for inverse s - 3
+            for i, (w, hx, hy, hz) in enumerate(host):
+                host[i] = (w, hx, hy + [torch.empty_like(hx, pin_memory=True)], hz)
         if args.e2e_schedule == "chains":
             for i, (w, hx, hy, hz) in enumerate(host):  # per chain its own intermediate and result
                 hy = hy + [torch.empty_like(hx, pin_memory=True) for _ in range(nchain - len(hy))]
@@ -772,12 +784,15 @@ def main():
                "matches_device_path": bool(same),
                "calls": "onefft_plan_forward/_inverse (single) and onefft_plan_forward/_inverse_batched (batch), "
                         "pinned host buffers",
-               "schedule": ("per item one forward and one inverse host thread; step s+1's forward overlaps "
-                            "step s's inverse (intermediates double-buffered); time of all steps / steps")
-               if args.e2e_schedule == "pairs" else
-               ("per item two host threads, each running whole steps (forward, then inverse) on its own "
-                "buffers, the second started one upload later so one uploads while the other downloads; "
-                "time of all steps / steps")}
+               "schedule": {"pairs": "per item one forward and one inverse host thread; step s+1's forward "
+                                     "overlaps step s's inverse (intermediates double-buffered); time of all "
+                                     "steps / steps",
+                            "offset": "per item one forward and one inverse host thread, the inverse thread "
+                                      "half a call behind (its uploads meet the forward thread's downloads); "
+                                      "three intermediates; time of all steps / steps",
+                            "chains": "per item two host threads, each running whole steps (forward, then "
+                                      "inverse) on its own buffers, the second started one upload later so one "
+                                      "uploads while the other downloads; time of all steps / steps"}[args.e2e_schedule]}
         for pf, pi in pools:
             pf.shutdown()
             pi.shutdown()
